@@ -1,0 +1,94 @@
+/*
+ * wavemoth_b200.h -- entry points of libwavemoth_b200.so beyond the
+ * reference's wavemoth.h: analysis (map2alm), device-pointer execution on a
+ * caller's CUDA stream, error reporting and test hooks.
+ *
+ * Conventions: functions returning int return 0 on success and a nonzero
+ * WAVEMOTH_ERR_* code otherwise; the message of the most recent failure on
+ * the calling thread is returned by wavemoth_last_error().  No function
+ * aborts the process.
+ */
+#ifndef WAVEMOTH_B200_H
+#define WAVEMOTH_B200_H
+
+#include "wavemoth.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* additive plan flags */
+#define WAVEMOTH_DEVICE_POINTERS 0x100   /* input/output given at plan time are device pointers */
+
+/* status codes */
+#define WAVEMOTH_OK 0
+#define WAVEMOTH_ERR_ARG 1         /* invalid argument or mismatched sizes */
+#define WAVEMOTH_ERR_RESOURCE 2    /* resource file missing, truncated or inconsistent */
+#define WAVEMOTH_ERR_CUDA 3        /* a CUDA call failed (message has the CUDA error) */
+#define WAVEMOTH_ERR_DEVICE 4      /* a kernel reported an error through its status word */
+#define WAVEMOTH_ERR_NOMEM 5       /* device allocation failed or exceeds the set memory cap */
+
+/* Message of the last failure on this thread ("" if none). */
+const char *wavemoth_last_error(void);
+
+/* Status of the last call made on the plan (WAVEMOTH_OK or an error code). */
+int wavemoth_plan_status(wavemoth_plan plan);
+
+/* map2alm plan: the analysis direction, defined as (4 pi / Npix) times the
+   adjoint of alm2map (a_lm = 4pi/Npix sum_p f_p lambda_lm(theta_p)
+   e^{-i m phi_p}).  Same signature as wavemoth_plan_to_healpix with the roles
+   of the buffers swapped: input = map (12 Nside^2, nmaps), output = alm
+   (nalm, nmaps) complex128.  No counterpart in the reference, which is
+   synthesis only; the analysis-direction Legendre step there is the GPU
+   prototype wavemoth/cuda/legendre_transform.cu.in:643-679. */
+wavemoth_plan wavemoth_plan_from_healpix(int Nside, int lmax, int mmax, int nmaps, int nthreads,
+                                         double *input, double *output, int ordering,
+                                         unsigned flags, char *resource_filename);
+
+/* Device-pointer execution on `stream` (a cudaStream_t; NULL = the plan's
+   own stream).  Asynchronous with respect to the host.  The plan's
+   intermediate buffers are shared by all calls on one plan, so calls on one
+   plan must not overlap in time (serialise them on one stream).
+   alm: (nalm, nmaps) complex128 as interleaved doubles; map: (npix, nmaps). */
+int wavemoth_execute_alm2map_device(wavemoth_plan plan, const double *alm, double *map,
+                                    void *stream);
+int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, double *alm,
+                                    void *stream);
+
+/* Copies the Legendre-phase output q (complex128, (mmax+1, 2, 2 Nside, nmaps))
+   to host memory `out`; the analogue of ShtPlan.get_work
+   (wavemoth/lib.pyx:158-179). */
+int wavemoth_get_work(wavemoth_plan plan, double *out);
+
+/* Plan geometry queries. */
+int wavemoth_plan_nmaps(wavemoth_plan plan);
+int wavemoth_plan_nside(wavemoth_plan plan);
+int wavemoth_plan_lmax(wavemoth_plan plan);
+/* Device bytes held by the plan (program arena + buffers). */
+int64_t wavemoth_plan_device_bytes(wavemoth_plan plan);
+/* Bytes of the compiled butterfly program (interpolants, recurrence data). */
+int64_t wavemoth_plan_program_bytes(wavemoth_plan plan);
+
+/* Caps the device memory a plan may allocate (bytes; <= 0 removes the cap).
+   Plans whose buffers would exceed it fail with WAVEMOTH_ERR_NOMEM.  Used to
+   exercise allocation-failure handling without exhausting the GPU. */
+void wavemoth_set_device_memory_cap(int64_t bytes);
+
+/* Parses and validates a rev1 file for (Nside, lmax) exactly as plan
+   creation does, without touching the GPU.  On success returns 0 and, if
+   out_stats is not NULL, fills out_stats[0..7] = (matrices, residual blocks,
+   strips, levels, interpolation pairs, f64 arena bytes, i32 arena bytes,
+   largest intermediate buffer rows).  No counterpart in the reference. */
+int wavemoth_check_resourcefile(char *filename, int Nside, int lmax, int64_t *out_stats);
+
+/* Host-side numerical tools of the plan-file writer (no GPU needed). */
+int wm_host_legendre(int m, const double *theta, int ntheta, int lmax, double eps, double *out);
+void wm_host_recurrence_coefficients(int64_t m, int64_t lmin, int64_t nk, double *aux);
+int wm_host_interp_decomp(double *A, int m, int n, double eps, int *krank, int *perm,
+                          double *proj);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

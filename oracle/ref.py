@@ -16,6 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(_HERE, "_ref", "libwavemoth_ref.so")
 _lib = None
+MAX_THREADS = 8
 
 
 def available():
@@ -54,6 +55,8 @@ def lib():
         L.refhook_legendre.argtypes = [ctypes.c_int, dp, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_double, dp]
         L.refhook_legendre.restype = ctypes.c_int
+        L.refhook_worker_sizes_ok.argtypes = [ctypes.c_void_p]
+        L.refhook_worker_sizes_ok.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -99,21 +102,34 @@ def query_resourcefile(path):
 
 
 class RefPlan:
-    def __init__(self, nside, lmax, nmaps, resource_file, nthreads=1, phase_shifts=True):
+    def __init__(self, nside, lmax, nmaps, resource_file, nthreads=1, phase_shifts=True,
+                 attempts=50):
         L = lib()
         self.nside, self.lmax, self.nmaps = nside, lmax, nmaps
         nalm = (lmax + 1) * (lmax + 2) // 2
         self.input = np.zeros((nalm, nmaps), np.complex128)
         self.output = np.zeros((12 * nside * nside, nmaps))
+        # one CPU per presented NUMA node, at most 8 nodes (see ref_hooks.c)
+        nthreads = max(1, min(int(nthreads), MAX_THREADS, len(os.sched_getaffinity(0))))
         self.nthreads = nthreads
         L.refhook_set_ncpus(nthreads)
-        with stdout_to_stderr():
-            self.plan = L.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, nthreads,
-                                                   _dp(self.input.view(np.float64)),
-                                                   _dp(self.output), 0, 0,
-                                                   resource_file.encode())
+        self.plan = None
+        for _ in range(attempts):
+            with stdout_to_stderr():
+                plan = L.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, nthreads,
+                                                  _dp(self.input.view(np.float64)),
+                                                  _dp(self.output), 0, 0,
+                                                  resource_file.encode())
+            if not plan:
+                raise RuntimeError("reference plan creation failed")
+            if L.refhook_worker_sizes_ok(plan):
+                self.plan = plan
+                break
+            # a worker lost the unsynchronised size reduction; this plan
+            # would trip the reference's own assert, so build it again
+            L.wavemoth_destroy_plan(plan)
         if not self.plan:
-            raise RuntimeError("reference plan creation failed")
+            raise RuntimeError("reference plan creation kept racing (%d attempts)" % attempts)
         if not phase_shifts:
             L.wavemoth_disable_phase_shifting(self.plan)
 

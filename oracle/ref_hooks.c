@@ -3,10 +3,16 @@
  * reference's own C sources into oracle/_ref/libwavemoth_ref.so.
  *
  *  1. FFTW3 entry points (declared in shims/fftw3.h) backed by oracle/fft.c.
- *  2. libnuma entry points (shims/numa.h).  The reference sizes its per-node
- *     CPU table for 16 CPUs (src/wavemoth.c:452), so the usable CPUs are
- *     presented as ceil(ncpus/16) nodes (at most 8, src/wavemoth_private.h:
- *     node_plans[8]) of up to 16 CPUs each.
+ *  2. libnuma entry points (shims/numa.h).  Every usable CPU is presented as
+ *     a NUMA node of its own (at most 8: src/wavemoth_private.h node_plans[8]).
+ *     With two or more CPUs on one node the reference's plan creation reduces
+ *     the per-node buffer sizes k_max / nblocks_max across threads with its
+ *     barriers commented out (src/wavemoth.c:766-783), and the thread that
+ *     first faults the resource in (icpu == 0, :690-727) resets the shared
+ *     value after the others have contributed; the workers then get buffers
+ *     that are too small and the reference's own assert
+ *     (src/butterfly.c.in:341) aborts.  One CPU per node is the only
+ *     configuration in which the unmodified reference plans reliably.
  *  3. Read-only accessors for plan internals that the reference's Cython
  *     layer reads directly: the Legendre-phase output work_q
  *     (wavemoth/lib.pyx:158-179, ShtPlan.get_work) and the phi0 table
@@ -63,7 +69,7 @@ void fftw_destroy_plan(fftw_plan p) {
 
 /* ---------------- libnuma shim ---------------- */
 #define OR_MASK_BITS 1024
-#define OR_CPUS_PER_NODE 16
+#define OR_CPUS_PER_NODE 1
 
 static int or_cpus[OR_MASK_BITS];
 static int or_ncpus = -1;
@@ -205,4 +211,30 @@ int refhook_legendre(int m, const double *theta, int ntheta, int lmax, double ep
   }
   Ylmgen_destroy(&ctx);
   return 0;
+}
+
+/* 1 if every Legendre worker's buffers (k_max, nblocks_max) are at least
+   the largest the matrices of its NUMA node need, else 0.
+   wavemoth_plan_to_healpix reduces these per node across the node's threads
+   without a barrier (src/wavemoth.c:766-783, barriers commented out); callers
+   recreate the plan when this returns 0 instead of letting the reference's
+   assert (src/butterfly.c.in:341) abort the process. */
+int refhook_worker_sizes_ok(wavemoth_plan plan) {
+  for (int inode = 0; inode < plan->nnodes; ++inode) {
+    wavemoth_node_plan_t *np = plan->node_plans[inode];
+    size_t need_k = 0, need_b = 0;
+    for (size_t im = 0; im < np->nm; ++im) {
+      for (int odd = 0; odd < 2; ++odd) {
+        bfm_matrix_data_info info;
+        bfm_query_matrix_data(np->m_resources[im].data[odd], &info);
+        if (info.k_max > need_k) need_k = info.k_max;
+        if (info.nblocks_max > need_b) need_b = info.nblocks_max;
+      }
+    }
+    for (int icpu = 0; icpu < np->ncpus; ++icpu) {
+      bfm_plan *b = np->cpu_plans[icpu].legendre_workers[0].bfm;
+      if (b->k_max < need_k || b->nblocks_max < need_b) return 0;
+    }
+  }
+  return 1;
 }

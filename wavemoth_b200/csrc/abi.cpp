@@ -1,0 +1,549 @@
+// C ABI of libwavemoth_b200.so: the plan object and every extern "C" entry
+// point declared in include/wavemoth.h and include/wavemoth_b200.h.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "plan.h"
+#include "program.h"
+#include "wavemoth.h"
+#include "wavemoth_b200.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::string g_resource_dir;
+int64_t g_device_cap = 0;
+
+int set_error(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+struct DeviceArena {
+  std::vector<void *> ptrs;
+  int64_t bytes = 0;
+  ~DeviceArena() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  int alloc(T **out, size_t count, const char *what) {
+    size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (g_device_cap > 0 && bytes + (int64_t)nbytes > g_device_cap)
+      return set_error(WAVEMOTH_ERR_NOMEM, std::string("device memory cap exceeded allocating ") + what);
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, nbytes);
+    if (e != cudaSuccess)
+      return set_error(WAVEMOTH_ERR_NOMEM, std::string("cudaMalloc(") + what + "): " +
+                                               cudaGetErrorString(e));
+    ptrs.push_back(p);
+    bytes += (int64_t)nbytes;
+    *out = (T *)p;
+    return 0;
+  }
+};
+
+}  // namespace
+
+struct _wavemoth_plan {
+  int nside = 0, lmax = 0, mmax = 0, nmaps = 0, nvecs = 0, ni = 0;
+  int64_t npix = 0, nalm = 0;
+  unsigned flags = 0;
+  bool analysis = false;          // map2alm plan
+  double *host_in = nullptr, *host_out = nullptr;
+  int status = 0;
+  int phase_shifts = 1;
+  int sm_count = 0;
+  int grid = 0;
+
+  wm::HostProgram prog;
+  DeviceArena arena;
+  int64_t program_bytes = 0;
+  wm::DevMatrix *d_mats = nullptr;
+  wm::DevDBlock *d_dblocks = nullptr;
+  wm::DevStrip *d_strips = nullptr;
+  wm::DevLevel *d_levels = nullptr;
+  wm::DevPair *d_pairs = nullptr;
+  double *d_f64 = nullptr;
+  int32_t *d_i32 = nullptr;
+  int32_t *d_order = nullptr;
+  int32_t *d_counter = nullptr;
+  wm::DevRing *d_rings = nullptr;
+  double *d_alm = nullptr, *d_map = nullptr, *d_q = nullptr, *d_scratch = nullptr;
+  int64_t slot_stride = 0;
+  cudaStream_t stream = nullptr;
+
+  ~_wavemoth_plan() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return 0;
+  return set_error(WAVEMOTH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+int upload(DeviceArena &A, T **dst, const std::vector<T> &src, const char *what) {
+  if (int rc = A.alloc(dst, src.size(), what)) return rc;
+  if (!src.empty())
+    return cuda_check(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice),
+                      what);
+  return 0;
+}
+
+bool read_file(const std::string &path, std::vector<char> &buf, std::string &err) {
+  FILE *f = fopen(path.c_str(), "rb");
+  if (!f) {
+    err = "cannot open resource file " + path;
+    return false;
+  }
+  fseek(f, 0, SEEK_END);
+  long n = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (n < 0) {
+    fclose(f);
+    err = "cannot size resource file " + path;
+    return false;
+  }
+  buf.resize((size_t)n);
+  size_t got = n ? fread(buf.data(), 1, (size_t)n, f) : 0;
+  fclose(f);
+  if (got != (size_t)n) {
+    err = "short read of resource file " + path;
+    return false;
+  }
+  return true;
+}
+
+std::vector<wm::DevRing> ring_table(int nside) {
+  const int nrings = 4 * nside - 1, mid = 2 * nside - 1;
+  std::vector<int64_t> offs(nrings + 1);
+  int64_t ipix = 0, npr = 0;
+  std::vector<int> num(nrings), den(nrings);
+  for (int r = 0; r < nrings; ++r) {
+    if (r <= nside - 1) {
+      npr += 4;
+      num[r] = 1;
+      den[r] = 4 * (r + 1);
+    } else if (r > 3 * nside - 1) {
+      npr -= 4;
+      num[r] = 1;
+      den[r] = 4 * (nrings - r);
+    } else {
+      num[r] = r % 2;
+      den[r] = 4 * nside;
+    }
+    offs[r] = ipix;
+    ipix += npr;
+  }
+  offs[nrings] = ipix;
+  std::vector<wm::DevRing> out(2 * nside);
+  for (int r = 0; r < 2 * nside; ++r) {
+    wm::DevRing R{};
+    R.n = (int32_t)(offs[mid + r + 1] - offs[mid + r]);
+    R.phi_num = num[mid + r];
+    R.phi_den = den[mid + r];
+    R.off_north = offs[mid - r];
+    R.off_south = offs[mid + r];
+    out[r] = R;
+  }
+  return out;
+}
+
+wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps, double *input,
+                        double *output, int ordering, unsigned flags, const char *resource_filename) {
+  if (nmaps <= 0 || lmax < 0 || mmax != lmax || ordering != WAVEMOTH_MMAJOR) {
+    set_error(WAVEMOTH_ERR_ARG, "invalid plan arguments (need nmaps > 0, mmax == lmax >= 0, "
+                                "ordering WAVEMOTH_MMAJOR)");
+    return nullptr;
+  }
+  std::string path;
+  if (resource_filename) {
+    path = resource_filename;
+  } else {
+    if (Nside <= 0 || g_resource_dir.empty()) {
+      set_error(WAVEMOTH_ERR_ARG, "no resource file given and wavemoth_configure not called");
+      return nullptr;
+    }
+    path = g_resource_dir + "/rev1/" + std::to_string(Nside) + ".dat";
+  }
+  std::vector<char> file;
+  std::string err;
+  if (!read_file(path, file, err)) {
+    set_error(WAVEMOTH_ERR_RESOURCE, err);
+    return nullptr;
+  }
+  auto *P = new _wavemoth_plan();
+  if (!wm::compile_resource(file.data(), file.size(), Nside, lmax, mmax, P->prog, err)) {
+    set_error(WAVEMOTH_ERR_RESOURCE, path + ": " + err);
+    delete P;
+    return nullptr;
+  }
+  file.clear();
+  file.shrink_to_fit();
+  P->nside = P->prog.nside;
+  P->lmax = lmax;
+  P->mmax = mmax;
+  P->nmaps = nmaps;
+  P->nvecs = 2 * nmaps;
+  P->ni = 2 * P->nside;
+  P->npix = 12LL * P->nside * P->nside;
+  P->nalm = (int64_t)(lmax + 1) * (lmax + 2) / 2;
+  P->flags = flags;
+  P->analysis = analysis;
+  P->host_in = input;
+  P->host_out = output;
+
+  int dev = 0;
+  if (cuda_check(cudaGetDevice(&dev), "cudaGetDevice") ||
+      cuda_check(cudaDeviceGetAttribute(&P->sm_count, cudaDevAttrMultiProcessorCount, dev),
+                 "cudaDeviceGetAttribute")) {
+    delete P;
+    return nullptr;
+  }
+  auto &G = P->prog;
+  // processing order: largest matrices first
+  std::vector<int32_t> order(G.mats.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return G.mats[a].cost > G.mats[b].cost; });
+  const int nmats = (int)G.mats.size();
+  P->grid = std::max(1, std::min(nmats, 2 * P->sm_count));
+  P->slot_stride = 2 * (int64_t)std::max<int32_t>(G.max_rows, 1) * P->nvecs;
+  int rc = 0;
+  DeviceArena &A = P->arena;
+  rc = rc ? rc : upload(A, &P->d_mats, G.mats, "matrices");
+  rc = rc ? rc : upload(A, &P->d_dblocks, G.dblocks, "residual blocks");
+  rc = rc ? rc : upload(A, &P->d_strips, G.strips, "strips");
+  rc = rc ? rc : upload(A, &P->d_levels, G.levels, "levels");
+  rc = rc ? rc : upload(A, &P->d_pairs, G.pairs, "pairs");
+  rc = rc ? rc : upload(A, &P->d_f64, G.f64, "f64 arena");
+  rc = rc ? rc : upload(A, &P->d_i32, G.i32, "i32 arena");
+  rc = rc ? rc : upload(A, &P->d_order, order, "order");
+  P->program_bytes = A.bytes;
+  rc = rc ? rc : upload(A, &P->d_rings, ring_table(P->nside), "ring table");
+  rc = rc ? rc : A.alloc(&P->d_counter, 1, "counter");
+  rc = rc ? rc : A.alloc(&P->d_q, (size_t)2 * (mmax + 1) * P->ni * P->nvecs, "q buffer");
+  rc = rc ? rc : A.alloc(&P->d_scratch, (size_t)P->grid * P->slot_stride, "butterfly scratch");
+  if (!(flags & WAVEMOTH_DEVICE_POINTERS)) {
+    rc = rc ? rc : A.alloc(&P->d_alm, (size_t)P->nalm * P->nvecs, "alm buffer");
+    rc = rc ? rc : A.alloc(&P->d_map, (size_t)P->npix * nmaps, "map buffer");
+  }
+  rc = rc ? rc : cuda_check(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking),
+                            "cudaStreamCreate");
+  if (rc) {
+    delete P;
+    return nullptr;
+  }
+  // host-side tables are no longer needed except element counts
+  G.dblocks.clear(); G.dblocks.shrink_to_fit();
+  G.strips.clear(); G.strips.shrink_to_fit();
+  G.pairs.clear(); G.pairs.shrink_to_fit();
+  G.f64.clear(); G.f64.shrink_to_fit();
+  G.i32.clear(); G.i32.shrink_to_fit();
+  return P;
+}
+
+wm::LegendreParams legendre_params(wavemoth_plan P) {
+  wm::LegendreParams p{};
+  p.mats = P->d_mats;
+  p.dblocks = P->d_dblocks;
+  p.strips = P->d_strips;
+  p.levels = P->d_levels;
+  p.pairs = P->d_pairs;
+  p.f64 = P->d_f64;
+  p.i32 = P->d_i32;
+  p.order = P->d_order;
+  p.nmats = (int32_t)P->prog.mats.size();
+  p.lmax = P->lmax;
+  p.nvecs = P->nvecs;
+  p.ni = P->ni;
+  p.scratch = P->d_scratch;
+  p.slot_stride = P->slot_stride;
+  p.counter = P->d_counter;
+  return p;
+}
+
+wm::RingParams ring_params(wavemoth_plan P) {
+  wm::RingParams r{};
+  r.rings = P->d_rings;
+  r.ni = P->ni;
+  r.nside = P->nside;
+  r.mmax = P->mmax;
+  r.nmaps = P->nmaps;
+  r.nvecs = P->nvecs;
+  r.scale = 4.0 * 3.14159265358979323846 / (double)P->npix;
+  r.phase_shifts = P->phase_shifts;
+  return r;
+}
+
+int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_out,
+                 const double *q_in, double *q_out, cudaStream_t st) {
+  wm::LegendreParams p = legendre_params(P);
+  p.alm_in = alm_in;
+  p.alm_out = alm_out;
+  p.q_in = q_in;
+  p.q_out = q_out;
+  if (int rc = cuda_check(cudaMemsetAsync(P->d_counter, 0, sizeof(int32_t), st), "counter reset"))
+    return rc;
+  return cuda_check(wm::launch_legendre(alm2map, p, P->grid, st), "Legendre kernel launch");
+}
+
+int run_alm2map(wavemoth_plan P, const double *alm, double *map, cudaStream_t st) {
+  if (int rc = run_legendre(P, true, alm, nullptr, nullptr, P->d_q, st)) return rc;
+  wm::RingParams r = ring_params(P);
+  r.q = P->d_q;
+  r.map = map;
+  return cuda_check(wm::launch_ring_synthesis(r, st), "ring synthesis launch");
+}
+
+int run_map2alm(wavemoth_plan P, const double *map, double *alm, cudaStream_t st) {
+  wm::RingParams r = ring_params(P);
+  r.map_in = map;
+  r.q_out = P->d_q;
+  if (int rc = cuda_check(wm::launch_ring_analysis(r, st), "ring analysis launch")) return rc;
+  return run_legendre(P, false, nullptr, alm, P->d_q, nullptr, st);
+}
+
+int finish(wavemoth_plan P, int rc) {
+  P->status = rc;
+  return rc;
+}
+
+int host_execute(wavemoth_plan P) {
+  cudaStream_t st = P->stream;
+  const bool devptr = (P->flags & WAVEMOTH_DEVICE_POINTERS) != 0;
+  const size_t alm_bytes = (size_t)P->nalm * P->nvecs * sizeof(double);
+  const size_t map_bytes = (size_t)P->npix * P->nmaps * sizeof(double);
+  if (!P->host_in || !P->host_out)
+    return set_error(WAVEMOTH_ERR_ARG, "plan has no bound input/output buffers");
+  int rc = 0;
+  if (!P->analysis) {
+    const double *alm = devptr ? P->host_in : P->d_alm;
+    double *map = devptr ? P->host_out : P->d_map;
+    if (!devptr)
+      rc = cuda_check(cudaMemcpyAsync(P->d_alm, P->host_in, alm_bytes, cudaMemcpyHostToDevice, st),
+                      "alm upload");
+    rc = rc ? rc : run_alm2map(P, alm, map, st);
+    if (!devptr && !rc)
+      rc = cuda_check(cudaMemcpyAsync(P->host_out, P->d_map, map_bytes, cudaMemcpyDeviceToHost, st),
+                      "map download");
+  } else {
+    const double *map = devptr ? P->host_in : P->d_map;
+    double *alm = devptr ? P->host_out : P->d_alm;
+    if (!devptr)
+      rc = cuda_check(cudaMemcpyAsync(P->d_map, P->host_in, map_bytes, cudaMemcpyHostToDevice, st),
+                      "map upload");
+    rc = rc ? rc : run_map2alm(P, map, alm, st);
+    if (!devptr && !rc)
+      rc = cuda_check(cudaMemcpyAsync(P->host_out, P->d_alm, alm_bytes, cudaMemcpyDeviceToHost, st),
+                      "alm download");
+  }
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(st), "execute");
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wavemoth_last_error(void) { return g_last_error.c_str(); }
+
+void wavemoth_configure(char *resource_dir) { g_resource_dir = resource_dir ? resource_dir : ""; }
+
+wavemoth_plan wavemoth_plan_to_healpix(int Nside, int lmax, int mmax, int nmaps, int nthreads,
+                                       double *input, double *output, int ordering,
+                                       unsigned flags, char *resource_filename) {
+  (void)nthreads;
+  return make_plan(false, Nside, lmax, mmax, nmaps, input, output, ordering, flags,
+                   resource_filename);
+}
+
+wavemoth_plan wavemoth_plan_from_healpix(int Nside, int lmax, int mmax, int nmaps, int nthreads,
+                                         double *input, double *output, int ordering,
+                                         unsigned flags, char *resource_filename) {
+  (void)nthreads;
+  return make_plan(true, Nside, lmax, mmax, nmaps, input, output, ordering, flags,
+                   resource_filename);
+}
+
+void wavemoth_destroy_plan(wavemoth_plan plan) {
+  if (!plan) return;
+  if (plan->stream) cudaStreamSynchronize(plan->stream);
+  delete plan;
+}
+
+void wavemoth_execute(wavemoth_plan plan) {
+  if (!plan) {
+    set_error(WAVEMOTH_ERR_ARG, "NULL plan");
+    return;
+  }
+  finish(plan, host_execute(plan));
+}
+
+int wavemoth_plan_status(wavemoth_plan plan) { return plan ? plan->status : WAVEMOTH_ERR_ARG; }
+
+int64_t wavemoth_get_legendre_flops(wavemoth_plan plan, int m, int odd) {
+  if (!plan || m < 0 || m > plan->mmax || odd < 0 || odd > 1) return -1;
+  return plan->prog.element_count[2 * m + odd] * 2 * 2;
+}
+
+int wavemoth_query_resourcefile(char *filename, int *out_Nside, int *out_lmax) {
+  if (!filename) return -1;
+  FILE *f = fopen(filename, "rb");
+  if (!f) return -1;
+  int64_t fields[3];
+  size_t got = fread(fields, sizeof(fields), 1, f);
+  fclose(f);
+  if (got != 1) {
+    set_error(WAVEMOTH_ERR_RESOURCE, std::string("could not read file header: ") + filename);
+    return -1;
+  }
+  *out_lmax = (int)fields[0];
+  *out_Nside = (int)fields[2];
+  return 0;
+}
+
+int wavemoth_execute_alm2map_device(wavemoth_plan plan, const double *alm, double *map,
+                                    void *stream) {
+  if (!plan || !alm || !map) return set_error(WAVEMOTH_ERR_ARG, "NULL plan or buffer");
+  cudaStream_t st = stream ? (cudaStream_t)stream : plan->stream;
+  return finish(plan, run_alm2map(plan, alm, map, st));
+}
+
+int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, double *alm,
+                                    void *stream) {
+  if (!plan || !alm || !map) return set_error(WAVEMOTH_ERR_ARG, "NULL plan or buffer");
+  cudaStream_t st = stream ? (cudaStream_t)stream : plan->stream;
+  return finish(plan, run_map2alm(plan, map, alm, st));
+}
+
+void wavemoth_perform_legendre_transforms(wavemoth_plan plan) {
+  if (!plan) return;
+  int rc = 0;
+  if (plan->analysis) {
+    rc = set_error(WAVEMOTH_ERR_ARG, "perform_legendre_transforms needs an alm2map plan");
+  } else if (plan->flags & WAVEMOTH_DEVICE_POINTERS) {
+    rc = run_legendre(plan, true, plan->host_in, nullptr, nullptr, plan->d_q, plan->stream);
+  } else {
+    rc = cuda_check(cudaMemcpyAsync(plan->d_alm, plan->host_in,
+                                    (size_t)plan->nalm * plan->nvecs * sizeof(double),
+                                    cudaMemcpyHostToDevice, plan->stream),
+                    "alm upload");
+    rc = rc ? rc : run_legendre(plan, true, plan->d_alm, nullptr, nullptr, plan->d_q, plan->stream);
+  }
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(plan->stream), "Legendre transforms");
+  finish(plan, rc);
+}
+
+void wavemoth_perform_backward_ffts(wavemoth_plan plan) {
+  if (!plan) return;
+  int rc = 0;
+  if (plan->analysis) {
+    rc = set_error(WAVEMOTH_ERR_ARG, "perform_backward_ffts needs an alm2map plan");
+  } else {
+    const bool devptr = (plan->flags & WAVEMOTH_DEVICE_POINTERS) != 0;
+    wm::RingParams r = ring_params(plan);
+    r.q = plan->d_q;
+    r.map = devptr ? plan->host_out : plan->d_map;
+    rc = cuda_check(wm::launch_ring_synthesis(r, plan->stream), "ring synthesis launch");
+    if (!rc && !devptr)
+      rc = cuda_check(cudaMemcpyAsync(plan->host_out, plan->d_map,
+                                      (size_t)plan->npix * plan->nmaps * sizeof(double),
+                                      cudaMemcpyDeviceToHost, plan->stream),
+                      "map download");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(plan->stream), "backward FFTs");
+  }
+  finish(plan, rc);
+}
+
+void wavemoth_disable_phase_shifting(wavemoth_plan plan) {
+  if (plan) plan->phase_shifts = 0;
+}
+
+int wavemoth_get_work(wavemoth_plan plan, double *out) {
+  if (!plan || !out) return set_error(WAVEMOTH_ERR_ARG, "NULL plan or buffer");
+  size_t n = (size_t)2 * (plan->mmax + 1) * plan->ni * plan->nvecs;
+  int rc = cuda_check(cudaMemcpyAsync(out, plan->d_q, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                      plan->stream), "work download");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(plan->stream), "work download");
+  return rc;
+}
+
+int wavemoth_plan_nmaps(wavemoth_plan plan) { return plan ? plan->nmaps : -1; }
+int wavemoth_plan_nside(wavemoth_plan plan) { return plan ? plan->nside : -1; }
+int wavemoth_plan_lmax(wavemoth_plan plan) { return plan ? plan->lmax : -1; }
+int64_t wavemoth_plan_device_bytes(wavemoth_plan plan) { return plan ? plan->arena.bytes : -1; }
+int64_t wavemoth_plan_program_bytes(wavemoth_plan plan) { return plan ? plan->program_bytes : -1; }
+
+void wavemoth_set_device_memory_cap(int64_t bytes) { g_device_cap = bytes; }
+
+int wavemoth_check_resourcefile(char *filename, int Nside, int lmax, int64_t *out_stats) {
+  if (!filename) return set_error(WAVEMOTH_ERR_ARG, "NULL file name");
+  std::vector<char> file;
+  std::string err;
+  if (!read_file(filename, file, err)) return set_error(WAVEMOTH_ERR_RESOURCE, err);
+  wm::HostProgram P;
+  if (!wm::compile_resource(file.data(), file.size(), Nside, lmax, lmax, P, err))
+    return set_error(WAVEMOTH_ERR_RESOURCE, std::string(filename) + ": " + err);
+  if (out_stats) {
+    out_stats[0] = (int64_t)P.mats.size();
+    out_stats[1] = (int64_t)P.dblocks.size();
+    out_stats[2] = (int64_t)P.strips.size();
+    out_stats[3] = (int64_t)P.levels.size();
+    out_stats[4] = (int64_t)P.pairs.size();
+    out_stats[5] = (int64_t)P.f64.size() * 8;
+    out_stats[6] = (int64_t)P.i32.size() * 4;
+    out_stats[7] = P.max_rows;
+  }
+  return 0;
+}
+
+wavemoth_grid_info *wavemoth_create_healpix_grid_info(int Nside) {
+  if (Nside <= 0 || Nside > (1 << 13)) {
+    set_error(WAVEMOTH_ERR_ARG, "invalid Nside");
+    return nullptr;
+  }
+  const int nrings = 4 * Nside - 1;
+  char *buf = (char *)malloc(sizeof(wavemoth_grid_info) + sizeof(double) * nrings +
+                             sizeof(bfm_index_t) * (nrings + 1));
+  if (!buf) return nullptr;
+  auto *g = (wavemoth_grid_info *)buf;
+  g->phi0s = (double *)(buf + sizeof(wavemoth_grid_info));
+  g->ring_offsets = (bfm_index_t *)(g->phi0s + nrings);
+  g->has_equator = 1;
+  g->nrings = nrings;
+  g->mid_ring = 2 * Nside - 1;
+  int npr = 0, ipix = 0;
+  const double pi = 3.14159265358979323846;
+  for (int r = 0; r < nrings; ++r) {
+    if (r <= Nside - 1) {
+      npr += 4;
+      g->phi0s[r] = pi / (4.0 * (r + 1));
+    } else if (r > 3 * Nside - 1) {
+      npr -= 4;
+      g->phi0s[r] = pi / (4.0 * (nrings - r));
+    } else {
+      g->phi0s[r] = (pi / (4.0 * Nside)) * (r % 2);
+    }
+    g->ring_offsets[r] = ipix;
+    ipix += npr;
+  }
+  g->ring_offsets[nrings] = ipix;
+  g->npix = ipix;
+  return g;
+}
+
+void wavemoth_free_grid_info(wavemoth_grid_info *info) { free(info); }
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// Device-side program of a butterfly-compressed Legendre transform.
+//
+// The host compiles every (m, parity) matrix of a rev1 resource file into
+// flat, level-major tables that live in one device arena:
+//
+//   DevMatrix  one per (m, parity): its residual blocks and its levels
+//   DevDBlock  one residual ("D") block of a forest root: rows
+//              [row_start, row_start + nrows) of the matrix (row k <-> l =
+//              m + parity + 2k) restricted to `ncols` skeleton columns, cut
+//              into strips
+//   DevStrip   columns [cstart, cstop) of a D block, rows [rstart, nrows):
+//              dense values or (x^2, P0, P1) for the three-term recurrence
+//   DevLevel   one tree depth: the interpolation pairs of every node at that
+//              depth, mapping the blocks of the upper (root-side) buffer to
+//              the blocks of the lower (leaf-side) buffer
+//   DevPair    the (T, B) interpolation blocks of one node pair slot
+//
+// State buffers: the blocks of all nodes at one tree depth are stored
+// back to back (heap order, then block order), `nvecs` doubles per row.  The
+// leaf depth buffer is the Legendre output q itself (rows = rings), so the
+// last level of alm2map writes q directly and the first level of map2alm
+// reads q~ directly.
+#pragma once
+#include <stdint.h>
+
+namespace wm {
+
+struct DevStrip {
+  int32_t rstart;   // first row (within the D block)
+  int32_t cstart;   // first column (within the D block)
+  int32_t cstop;
+  int32_t kind;     // 0: dense (nrows - rstart) x (cstop - cstart), column-major; 1: recurrence
+  int32_t dblock;   // owning residual block
+  int32_t pad;
+  int64_t data;     // f64 arena offset; recurrence: x2[nx], P0[nx], P1[nx]
+};
+
+struct DevDBlock {
+  int32_t row_start;
+  int32_t nrows;
+  int32_t ncols;
+  int32_t out_row;      // first row of this block in the depth-0 buffer
+  int32_t strip_begin;
+  int32_t strip_end;
+  int64_t aux;          // f64 arena offset of 3*(nrows-2) recurrence coefficients
+};
+
+struct DevPair {
+  int32_t kT, kB, n, n_left;
+  int32_t inT, inB;            // rows of the skeleton blocks in the upper buffer
+  int32_t out_left, out_right; // rows of the children's blocks in the lower buffer
+  int64_t mapT, mapB;          // i32 arena, n entries: >= 0 interpolant column, < 0: -(1 + skeleton row)
+  int64_t permT, permB;        // i32 arena, n entries: z positions of skeleton rows, then of columns
+  int64_t ipT, ipB;            // f64 arena: k x (n-k) column-major
+  int64_t ipT_t, ipB_t;        // f64 arena: (n-k) x k column-major (transposed copy)
+};
+
+struct DevLevel {
+  int32_t pair_begin, pair_end;
+  int32_t upper_rows, lower_rows;
+  int64_t lower_map;     // i32 arena, 2 per lower row: (pair index, z = row within the pair's n)
+  int64_t upper_map;     // i32 arena, 2 per upper row: (pair index, s >= 0 row of T, < 0: -(1+s) of B)
+};
+
+struct DevMatrix {
+  int32_t m, odd, nk, ncols;
+  int32_t nlevels;
+  int32_t dblock_begin, dblock_end;
+  int32_t level_begin;   // level_begin + t = tree depth t (0 = forest roots)
+  int32_t root_rows;     // rows of the depth-0 buffer
+  int32_t max_rows;      // rows of the largest intermediate buffer
+  int64_t root_map;      // i32 arena, 2 per depth-0 row: (strip index, column within the strip)
+  double cost;           // estimated work, for scheduling
+};
+
+// Per ring pair (ring number r from the equator).
+struct DevRing {
+  int32_t n;              // pixels in the ring
+  int32_t phi_num;        // phi0 = pi * phi_num / phi_den
+  int32_t phi_den;
+  int32_t pad;
+  int64_t off_north;      // first pixel of ring mid - r
+  int64_t off_south;      // first pixel of ring mid + r (== off_north at the equator)
+};
+
+// Device-resident error word (never trap: kernels record and return).
+enum : int32_t {
+  kStatusOk = 0,
+  kStatusBadProgram = 1,   // a table entry out of range
+  kStatusTimeout = 2,      // a bounded wait gave up
+};
+
+}  // namespace wm

@@ -1,0 +1,434 @@
+// rev1 resource file -> flat device program (plan.h).
+//
+// The rev1 layout read here is the reference's (src/wavemoth.c:203-264 for
+// the file header, src/butterfly.c.in:284-445 and src/butterfly.h.in:8-88 for
+// one matrix, src/wavemoth.c:958-1009 for a residual payload).  Unlike the
+// reference reader, every offset, count and size is range-checked against
+// the file so that a truncated or corrupt file yields an error message, not
+// a crash.
+#include <stdint.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+#include "program.h"
+
+namespace wm {
+
+namespace {
+
+struct Reader {
+  const char *base;
+  size_t len;
+  std::string *err;
+  bool ok = true;
+
+  bool fail(const std::string &msg) {
+    if (ok) *err = msg;
+    ok = false;
+    return false;
+  }
+  bool check(size_t off, size_t n, const char *what) {
+    if (off > len || n > len - off) return fail(std::string("resource file truncated: ") + what);
+    return true;
+  }
+  template <class T>
+  T get(size_t off, const char *what) {
+    T v{};
+    if (check(off, sizeof(T), what)) memcpy(&v, base + off, sizeof(T));
+    return v;
+  }
+};
+
+inline size_t pad16(size_t off) { return (off + 15) & ~size_t(15); }
+
+struct NodeInfo {
+  bool present = false;
+  int32_t nblocks = 0;           // 0 for a leaf
+  std::vector<int32_t> heights;  // leaf: {n}
+  size_t data = 0;               // file offset just after the heights
+};
+
+size_t append_f64(std::vector<double> &arena, const char *src, size_t n) {
+  size_t off = (arena.size() + 3) & ~size_t(3);
+  arena.resize(off + n);
+  if (n) memcpy(arena.data() + off, src, n * sizeof(double));
+  return off;
+}
+
+size_t append_i32(std::vector<int32_t> &arena, const std::vector<int32_t> &v) {
+  size_t off = (arena.size() + 3) & ~size_t(3);
+  arena.resize(off + v.size());
+  std::copy(v.begin(), v.end(), arena.begin() + off);
+  return off;
+}
+
+bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int ncols_expect,
+                    HostProgram &P) {
+  if (start % 16 != 0) return R.fail("matrix data not 16-byte aligned");
+  int32_t nrows = R.get<int32_t>(start + 0, "matrix header");
+  int32_t ncols = R.get<int32_t>(start + 4, "matrix header");
+  int64_t element_count = R.get<int64_t>(start + 16, "matrix header");
+  int32_t nroots = R.get<int32_t>(start + 24, "matrix header");
+  int32_t heap_size = R.get<int32_t>(start + 28, "matrix header");
+  int32_t heap_first = R.get<int32_t>(start + 32, "matrix header");
+  if (!R.ok) return false;
+  char buf[256];
+  if (ncols != ncols_expect || nrows != nk_expect) {
+    snprintf(buf, sizeof buf, "matrix m=%d odd=%d has shape %dx%d, expected %dx%d", m, odd, nrows,
+             ncols, nk_expect, ncols_expect);
+    return R.fail(buf);
+  }
+  if (nroots <= 0 || heap_size < nroots || heap_first < 1 || heap_first > (1 << 24) ||
+      heap_size > (1 << 24))
+    return R.fail("matrix header has an invalid forest/heap description");
+  size_t table = start + 40;
+  std::vector<int64_t> res_off(nroots), heap_off(heap_size);
+  for (int i = 0; i < nroots; ++i) res_off[i] = R.get<int64_t>(table + 8 * i, "residual table");
+  for (int i = 0; i < heap_size; ++i)
+    heap_off[i] = R.get<int64_t>(table + 8 * (nroots + i), "heap table");
+  if (!R.ok) return false;
+
+  auto node = [&](int64_t pos, NodeInfo &ni) -> bool {
+    int64_t idx = pos - heap_first;
+    if (idx < 0 || idx >= heap_size) return R.fail("heap position out of range");
+    if (heap_off[idx] <= 0) return R.fail("missing heap node");
+    size_t off = start + (size_t)heap_off[idx];
+    ni.present = true;
+    ni.nblocks = R.get<int32_t>(off, "node");
+    if (ni.nblocks < 0 || ni.nblocks > (1 << 20)) return R.fail("invalid node block count");
+    if (ni.nblocks == 0) {
+      ni.heights = {R.get<int32_t>(off + 4, "leaf node")};
+      ni.data = off + 8;
+    } else {
+      ni.heights.resize(ni.nblocks);
+      if (!R.check(off + 4, 4 * (size_t)ni.nblocks, "node heights")) return false;
+      memcpy(ni.heights.data(), R.base + off + 4, 4 * (size_t)ni.nblocks);
+      ni.data = off + 4 + 4 * (size_t)ni.nblocks;
+    }
+    for (int32_t h : ni.heights)
+      if (h < 0 || h > (1 << 24)) return R.fail("invalid block height");
+    return R.ok;
+  };
+
+  // depth of the forest (all roots of a complete tree have the same depth)
+  int depth = 0;
+  {
+    int64_t p = heap_first;
+    NodeInfo ni;
+    for (;;) {
+      if (!node(p, ni)) return false;
+      if (ni.nblocks == 0) break;
+      ++depth;
+      p *= 2;
+      if (depth > 30) return R.fail("tree too deep");
+    }
+  }
+  // nodes per depth, and row offsets of every block in that depth's buffer
+  std::vector<std::vector<NodeInfo>> nodes(depth + 1);
+  std::vector<std::vector<std::vector<int32_t>>> offs(depth + 1);
+  std::vector<int32_t> rows_at(depth + 1, 0);
+  for (int d = 0; d <= depth; ++d) {
+    int64_t p0 = (int64_t)heap_first << d, p1 = ((int64_t)heap_first + nroots) << d;
+    nodes[d].resize(p1 - p0);
+    offs[d].resize(p1 - p0);
+    int64_t row = 0;
+    for (int64_t p = p0; p < p1; ++p) {
+      NodeInfo &ni = nodes[d][p - p0];
+      if (!node(p, ni)) return false;
+      if ((d < depth) != (ni.nblocks > 0)) return R.fail("butterfly tree is not complete");
+      for (int32_t h : ni.heights) {
+        offs[d][p - p0].push_back((int32_t)row);
+        row += h;
+      }
+      if (row > (1 << 28)) return R.fail("butterfly buffer too large");
+    }
+    rows_at[d] = (int32_t)row;
+  }
+  if (rows_at[depth] != ncols) return R.fail("leaf widths do not add up to the column count");
+
+  DevMatrix M{};
+  M.m = m;
+  M.odd = odd;
+  M.nk = nrows;
+  M.ncols = ncols;
+  M.nlevels = depth;
+  M.dblock_begin = (int32_t)P.dblocks.size();
+  M.level_begin = (int32_t)P.levels.size();
+  M.root_rows = rows_at[0];
+  M.max_rows = 0;
+  for (int d = 0; d < depth; ++d) M.max_rows = std::max(M.max_rows, rows_at[d]);
+  double cost = 0;
+
+  // ---- interpolation levels ----
+  for (int d = 0; d < depth; ++d) {
+    DevLevel L{};
+    L.pair_begin = (int32_t)P.pairs.size();
+    L.upper_rows = rows_at[d];
+    L.lower_rows = rows_at[d + 1];
+    int64_t p0 = (int64_t)heap_first << d;
+    for (size_t u = 0; u < nodes[d].size(); ++u) {
+      const NodeInfo &ni = nodes[d][u];
+      int64_t p = p0 + (int64_t)u;
+      size_t cl = (size_t)(2 * p - ((int64_t)heap_first << (d + 1)));
+      const NodeInfo &lc = nodes[d + 1][cl], &rc = nodes[d + 1][cl + 1];
+      int npairs = ni.nblocks / 2;
+      if (ni.nblocks % 2 != 0 || (int)lc.heights.size() != npairs ||
+          (int)rc.heights.size() != npairs)
+        return R.fail("children do not match the parent's block count");
+      size_t off = ni.data;
+      for (int i = 0; i < npairs; ++i) {
+        DevPair pr{};
+        pr.n_left = lc.heights[i];
+        int32_t n = lc.heights[i] + rc.heights[i];
+        pr.n = n;
+        pr.out_left = offs[d + 1][cl][i];
+        pr.out_right = offs[d + 1][cl + 1][i];
+        for (int j = 0; j < 2; ++j) {
+          int32_t k = ni.heights[2 * i + j];
+          if (k > n) return R.fail("interpolation block has more rows than columns");
+          if (!R.check(off, (size_t)n, "filter")) return false;
+          const int8_t *filt = (const int8_t *)(R.base + off);
+          std::vector<int32_t> map(n), perm(n);
+          int zeros = 0, ones = 0;
+          for (int z = 0; z < n; ++z)
+            if (filt[z] == 0) ++zeros;
+            else if (filt[z] == 1) ++ones;
+            else return R.fail("filter entry not 0/1");
+          if (zeros != k) return R.fail("filter does not select k skeleton columns");
+          int s = 0, c = 0;
+          for (int z = 0; z < n; ++z) {
+            if (filt[z] == 0) { map[z] = -(1 + s); perm[s] = z; ++s; }
+            else { map[z] = c; perm[k + c] = z; ++c; }
+          }
+          off = pad16(off + n);
+          size_t nel = (size_t)k * (size_t)(n - k);
+          if (!R.check(off, 8 * nel, "interpolant")) return false;
+          const double *ip = (const double *)(R.base + off);
+          off += 8 * nel;
+          size_t ipo = append_f64(P.f64, (const char *)ip, nel);
+          // transposed copy: (n-k) x k column-major
+          std::vector<double> tr(nel);
+          for (int c2 = 0; c2 < n - k; ++c2)
+            for (int s2 = 0; s2 < k; ++s2) tr[c2 + (size_t)s2 * (n - k)] = ip[s2 + (size_t)c2 * k];
+          size_t ipt = append_f64(P.f64, (const char *)tr.data(), nel);
+          size_t mo = append_i32(P.i32, map), po = append_i32(P.i32, perm);
+          if (j == 0) {
+            pr.kT = k; pr.inT = offs[d][u][2 * i]; pr.mapT = mo; pr.permT = po;
+            pr.ipT = ipo; pr.ipT_t = ipt;
+          } else {
+            pr.kB = k; pr.inB = offs[d][u][2 * i + 1]; pr.mapB = mo; pr.permB = po;
+            pr.ipB = ipo; pr.ipB_t = ipt;
+          }
+          cost += (double)nel + n;
+        }
+        P.pairs.push_back(pr);
+      }
+    }
+    L.pair_end = (int32_t)P.pairs.size();
+    std::vector<int32_t> lower(2 * (size_t)L.lower_rows, -1), upper(2 * (size_t)L.upper_rows, -1);
+    for (int32_t pi = L.pair_begin; pi < L.pair_end; ++pi) {
+      const DevPair &pr = P.pairs[pi];
+      for (int32_t z = 0; z < pr.n; ++z) {
+        int32_t row = z < pr.n_left ? pr.out_left + z : pr.out_right + (z - pr.n_left);
+        if (row < 0 || row >= L.lower_rows || lower[2 * row] != -1)
+          return R.fail("interpolation pairs do not tile the lower buffer");
+        lower[2 * row] = pi;
+        lower[2 * row + 1] = z;
+      }
+      for (int32_t s = 0; s < pr.kT + pr.kB; ++s) {
+        int32_t row = s < pr.kT ? pr.inT + s : pr.inB + (s - pr.kT);
+        if (row < 0 || row >= L.upper_rows || upper[2 * row] != -1)
+          return R.fail("interpolation pairs do not tile the upper buffer");
+        upper[2 * row] = pi;
+        upper[2 * row + 1] = s < pr.kT ? s : -(1 + (s - pr.kT));
+      }
+    }
+    for (size_t i = 0; i < lower.size(); i += 2)
+      if (lower[i] == -1) {
+        snprintf(buf, sizeof buf, "m=%d odd=%d depth %d: lower buffer row %zu of %d not produced",
+                 m, odd, d, i / 2, L.lower_rows);
+        return R.fail(buf);
+      }
+    for (size_t i = 0; i < upper.size(); i += 2)
+      if (upper[i] == -1) {
+        snprintf(buf, sizeof buf, "m=%d odd=%d depth %d: upper buffer row %zu of %d not consumed",
+                 m, odd, d, i / 2, L.upper_rows);
+        return R.fail(buf);
+      }
+    L.lower_map = (int64_t)append_i32(P.i32, lower);
+    L.upper_map = (int64_t)append_i32(P.i32, upper);
+    P.levels.push_back(L);
+  }
+
+  // ---- residual blocks of every forest root ----
+  for (int r = 0; r < nroots; ++r) {
+    const NodeInfo &root = nodes[0][r];
+    int nb = (int)root.heights.size();
+    if (res_off[r] <= 0) return R.fail("missing residual payload table");
+    size_t toff = start + (size_t)res_off[r];
+    int64_t n = R.get<int64_t>(toff, "residual payload table");
+    if (!R.ok) return false;
+    if (n != nb) return R.fail("residual payload count does not match the root");
+    std::vector<int64_t> po(n + 1);
+    for (int64_t j = 0; j <= n; ++j) po[j] = R.get<int64_t>(toff + 8 + 8 * j, "payload offsets");
+    if (!R.ok) return false;
+    for (int j = 0; j < nb; ++j) {
+      DevDBlock D{};
+      D.ncols = root.heights[j];
+      D.out_row = offs[0][r][j];
+      D.strip_begin = (int32_t)P.strips.size();
+      D.aux = -1;
+      size_t off = pad16(start + (size_t)po[j]);
+      int64_t rs = R.get<int64_t>(off, "payload"), re = R.get<int64_t>(off + 8, "payload");
+      if (!R.ok) return false;
+      if (rs < 0 || re < rs || re > nrows) return R.fail("payload row range outside the matrix");
+      off += 16;
+      D.row_start = (int32_t)rs;
+      D.nrows = (int32_t)(re - rs);
+      int32_t nkb = D.nrows;
+      if (nkb <= 4 || D.ncols == 0) {
+        off = pad16(off);
+        size_t nel = (size_t)nkb * D.ncols;
+        if (!R.check(off, 8 * nel, "dense residual block")) return false;
+        DevStrip S{0, 0, D.ncols, 0, (int32_t)P.dblocks.size(), 0,
+                   (int64_t)append_f64(P.f64, R.base + off, nel)};
+        P.strips.push_back(S);
+        cost += (double)nel;
+      } else {
+        int64_t nstrips = R.get<int64_t>(off, "strip count");
+        off += 8;
+        if (!R.ok) return false;
+        if (nstrips <= 0 || nstrips > D.ncols + 1) return R.fail("invalid strip count");
+        off = pad16(off);
+        size_t naux = 3 * (size_t)(nkb - 2);
+        if (!R.check(off, 8 * naux, "recurrence coefficients")) return false;
+        D.aux = (int64_t)append_f64(P.f64, R.base + off, naux);
+        off += 8 * naux;
+        int32_t cstart = 0;
+        for (int64_t s = 0; s < nstrips; ++s) {
+          int64_t rstart = R.get<int64_t>(off, "strip"), cstop = R.get<int64_t>(off + 8, "strip");
+          off += 16;
+          if (!R.ok) return false;
+          if (rstart < 0 || rstart > nkb || cstop < cstart || cstop > D.ncols)
+            return R.fail("strip outside its residual block");
+          int32_t nx = (int32_t)cstop - cstart, nks = nkb - (int32_t)rstart;
+          DevStrip S{(int32_t)rstart, cstart, (int32_t)cstop, 0, (int32_t)P.dblocks.size(), 0, 0};
+          if (nks <= 4) {
+            off = pad16(off);
+            size_t nel = (size_t)nks * nx;
+            if (!R.check(off, 8 * nel, "dense strip")) return false;
+            S.data = (int64_t)append_f64(P.f64, R.base + off, nel);
+            off += 8 * nel;
+          } else {
+            S.kind = 1;
+            size_t o[3];
+            for (int a = 0; a < 3; ++a) {
+              off = pad16(off);
+              if (!R.check(off, 8 * (size_t)nx, "recurrence strip")) return false;
+              o[a] = off;
+              off += 8 * (size_t)nx;
+            }
+            // keep x2, P0, P1 contiguous
+            size_t base = (P.f64.size() + 3) & ~size_t(3);
+            P.f64.resize(base + 3 * (size_t)nx);
+            for (int a = 0; a < 3; ++a)
+              memcpy(P.f64.data() + base + (size_t)a * nx, R.base + o[a], 8 * (size_t)nx);
+            S.data = (int64_t)base;
+          }
+          cost += (double)nks * nx * (S.kind ? 2.5 : 1.0);
+          P.strips.push_back(S);
+          cstart = (int32_t)cstop;
+        }
+        if (cstart != D.ncols) return R.fail("strips do not cover the residual block");
+      }
+      D.strip_end = (int32_t)P.strips.size();
+      P.dblocks.push_back(D);
+    }
+  }
+  M.dblock_end = (int32_t)P.dblocks.size();
+  {
+    std::vector<int32_t> rm(2 * (size_t)M.root_rows, -1);
+    for (int32_t b = M.dblock_begin; b < M.dblock_end; ++b) {
+      const DevDBlock &D = P.dblocks[b];
+      for (int32_t s = D.strip_begin; s < D.strip_end; ++s) {
+        const DevStrip &S = P.strips[s];
+        for (int32_t c = S.cstart; c < S.cstop; ++c) {
+          int32_t row = D.out_row + c;
+          if (row < 0 || row >= M.root_rows || rm[2 * row] != -1)
+            return R.fail("residual blocks do not tile the root buffer");
+          rm[2 * row] = s;
+          rm[2 * row + 1] = c - S.cstart;
+        }
+      }
+    }
+    for (int32_t v : rm)
+      if (v == -1) return R.fail("root buffer row not produced by any residual block");
+    M.root_map = (int64_t)append_i32(P.i32, rm);
+  }
+  M.cost = cost;
+  P.element_count[2 * m + odd] = element_count;
+  P.mats.push_back(M);
+  return R.ok;
+}
+
+}  // namespace
+
+bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_expect,
+                      int mmax_expect, HostProgram &P, std::string &err) {
+  Reader R{data, len, &err};
+  int64_t lmax = R.get<int64_t>(0, "file header");
+  int64_t mmax = R.get<int64_t>(8, "file header");
+  int64_t nside = R.get<int64_t>(16, "file header");
+  if (!R.ok) return false;
+  char buf[256];
+  if (nside_expect >= 0 && nside != nside_expect) {
+    snprintf(buf, sizeof buf, "Incompatible Nside: file has %lld, plan wants %d", (long long)nside,
+             nside_expect);
+    err = buf;
+    return false;
+  }
+  if (lmax != lmax_expect || mmax != mmax_expect) {
+    snprintf(buf, sizeof buf, "Incompatible lmax/mmax: file has %lld/%lld, plan wants %d/%d",
+             (long long)lmax, (long long)mmax, lmax_expect, mmax_expect);
+    err = buf;
+    return false;
+  }
+  if (nside <= 0 || nside > (1 << 15) || lmax < 0 || mmax > lmax) {
+    err = "invalid file header";
+    return false;
+  }
+  P.nside = (int)nside;
+  P.lmax = (int)lmax;
+  P.mmax = (int)mmax;
+  P.element_count.assign(2 * (mmax + 1), 0);
+  const int ncols = 2 * (int)nside;
+  for (int m = 0; m <= mmax; ++m) {
+    for (int odd = 0; odd < 2; ++odd) {
+      int64_t start = R.get<int64_t>(24 + 8 * (4 * m + 2 * odd), "offset table");
+      int64_t mlen = R.get<int64_t>(24 + 8 * (4 * m + 2 * odd + 1), "offset table");
+      if (!R.ok) return false;
+      int nk = std::max(0, ((int)lmax - m - odd) / 2 + 1);
+      if (lmax - m - odd < 0) nk = 0;
+      if (start == 0) {
+        snprintf(buf, sizeof buf, "matrix m=%d odd=%d missing from resource file", m, odd);
+        err = buf;
+        return false;
+      }
+      if (start < 0 || mlen < 0 || (size_t)start > len || (size_t)mlen > len - (size_t)start) {
+        snprintf(buf, sizeof buf, "matrix m=%d odd=%d lies outside the resource file", m, odd);
+        err = buf;
+        return false;
+      }
+      Reader Rm{data, (size_t)start + (size_t)mlen, &err};
+      if (!compile_matrix(Rm, (size_t)start, m, odd, nk, ncols, P)) return false;
+    }
+  }
+  P.max_rows = 0;
+  for (auto &M : P.mats) P.max_rows = std::max(P.max_rows, M.max_rows);
+  return true;
+}
+
+}  // namespace wm
