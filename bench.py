@@ -1,0 +1,435 @@
+"""Benchmark: alm2map + map2alm round trips on HEALPix, maps per second.
+
+Workload (default): nside 1024, lmax = mmax = 2048, 32 maps per step; alm
+re/im iid N(0,1)(l+1)^-1 (Im = 0 at m = 0), one seeded generator per map;
+the butterfly plan file is written by wavemoth_b200.resource (ID eps 1e-10,
+chunk 64, memop cost 20) into the plan cache before anything is timed.
+A step = alm2map of the batch followed by map2alm of the resulting maps.
+
+Contract: ``python bench.py --gpus N --steps K --warmup W``; N > 1 runs
+under torch.distributed.run with one rank per GPU, each rank processing its
+own batch of maps (weak scaling, no data-path collective: the maps of a batch
+are independent).  Rank 0 prints one JSON line.  ``--impl reference`` times
+the reference's own C implementation (oracle/_ref) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "alm2map+map2alm maps/sec nside=1024 lmax=2048: batched/split vs plain FP64 at ≤1e-9"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nside", type=int, default=1024)
+    ap.add_argument("--lmax", type=int, default=None)
+    ap.add_argument("--nmaps", type=int, default=32)
+    ap.add_argument("--eps", type=float, default=1e-10)
+    ap.add_argument("--chunk", type=int, default=64)
+    ap.add_argument("--memop", type=float, default=20.0)
+    ap.add_argument("--plan-dir", default=os.environ.get("WAVEMOTH_PLAN_DIR",
+                                                         os.path.join(ROOT, ".plan_cache")))
+    ap.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--check", action="store_true",
+                    help="also report the round-trip relative error of map 0 vs the FP64 oracle "
+                         "at a reduced size (slow on CPU)")
+    a = ap.parse_args()
+    if a.lmax is None:
+        a.lmax = 2 * a.nside
+    return a
+
+
+def log(*args):
+    print(*args, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------- plan
+
+def plan_path(a):
+    return os.path.join(a.plan_dir, "rev1_nside%d_lmax%d_eps%g_chunk%d_memop%g.dat"
+                        % (a.nside, a.lmax, a.eps, a.chunk, a.memop))
+
+
+def ensure_plan(a, rank):
+    from wavemoth_b200 import resource
+    path = plan_path(a)
+    if os.path.exists(path):
+        return path
+    if rank == 0:
+        os.makedirs(a.plan_dir, exist_ok=True)
+        t = time.time()
+        log("writing plan file %s ..." % path)
+        resource.compute_resource_file(path, a.nside, a.lmax, chunk_size=a.chunk, eps=a.eps,
+                                       memop_cost=a.memop)
+        log("plan written in %.1f s" % (time.time() - t))
+        return path
+    deadline = time.time() + 1800
+    while not os.path.exists(path):
+        if time.time() > deadline:
+            raise TimeoutError("rank %d: plan file never appeared" % rank)
+        time.sleep(2)
+    return path
+
+
+def synthetic_alm(lmax, nmaps, seed0, power=1.0):
+    """complex128 (nalm, nmaps); map k uses its own generator seeded seed0 + k."""
+    ls = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    ms = np.concatenate([np.full(lmax - m + 1, m) for m in range(lmax + 1)])
+    scale = (ls + 1.0) ** -power
+    out = np.empty((ls.shape[0], nmaps), np.complex128)
+    for k in range(nmaps):
+        g = np.random.default_rng(seed0 + k)
+        re = g.standard_normal(ls.shape[0])
+        im = g.standard_normal(ls.shape[0])
+        im[ms == 0] = 0.0
+        out[:, k] = (re + 1j * im) * scale
+    return out
+
+
+# ------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        loaded = [s for s in sm if smax and s > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU baseline
+
+class ReferenceRunner:
+    """The reference's own C alm2map (oracle/_ref, built from its sources)
+    on the host cores, with as many threads as its plan code runs reliably
+    (one per presented NUMA node, at most 8).  The reference has no map2alm;
+    a round trip is costed as two alm2map executes (the adjoint performs the
+    same multiply-adds over the same compressed matrices)."""
+
+    def __init__(self, a, path, nmaps=4):
+        from oracle import ref
+        self.nmaps = nmaps
+        self.threads = max(1, min(ref.MAX_THREADS, len(os.sched_getaffinity(0))))
+        with ref.stdout_to_stderr():
+            self.rp = ref.RefPlan(a.nside, a.lmax, nmaps, path, nthreads=self.threads)
+        self.rp.input[:] = synthetic_alm(a.lmax, nmaps, 1000)
+
+    def execute(self):
+        t0 = time.perf_counter()
+        self.rp.execute()
+        return time.perf_counter() - t0
+
+    def rate(self, t):
+        return self.nmaps / (2.0 * t)
+
+    def describe(self, n):
+        return ("reference C alm2map (wavemoth_execute; FFT through the oracle's shim, not "
+                "FFTW), %d maps per execute, %d thread(s); best of %d executes after warm-up; "
+                "round trip costed as 2 alm2map (the reference has no map2alm)"
+                % (self.nmaps, self.threads, n))
+
+    def close(self):
+        self.rp.close()
+
+
+def reference_rate(a, path, seconds):
+    r = ReferenceRunner(a, path)
+    r.execute()  # warm-up: page-in and first touch
+    times = []
+    t_end = time.time() + seconds
+    while True:
+        times.append(r.execute())
+        if time.time() > t_end:
+            break
+    best = min(times)
+    out = {"value": r.rate(best), "unit": "maps/s", "cores": r.threads, "kind": "reference",
+           "sample": r.describe(len(times)), "seconds_per_execute": best}
+    r.close()
+    return out
+
+
+# --------------------------------------------------------------- GPU arm
+
+def fp64_peak_tflops(torch):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    return None
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+    from wavemoth_b200.sht import Transform
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    path = ensure_plan(a, rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    t0 = time.time()
+    T = Transform(path, a.nside, a.lmax, a.nmaps)
+    log("plan loaded in %.1f s" % (time.time() - t0))
+    work = T.work()
+    alm_h = synthetic_alm(a.lmax, a.nmaps, 1000 + rank * a.nmaps)
+    alm = torch.from_numpy(alm_h).cuda()
+    maps = torch.empty((T.npix, a.nmaps), dtype=torch.float64, device="cuda")
+    alm_out = torch.empty_like(alm)
+
+    def step(src):
+        T.alm2map(src, out=maps)
+        T.map2alm(maps, out=alm_out)
+
+    for _ in range(a.warmup):
+        step(alm)
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timing ----------------
+    T.timing(1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        step(alm)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    kt = T.timing(2)
+    T.timing(0)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / a.steps
+    value = world * a.nmaps * a.steps / (ms / 1e3)
+
+    # ---------------- end to end (host buffers) ----------------
+    e2e = None
+    if not a.no_e2e:
+        h_in = torch.from_numpy(alm_h).pin_memory()
+        h_out = torch.empty_like(h_in).pin_memory()
+        d_in = torch.empty_like(alm)
+        st = torch.cuda.current_stream()
+        for _ in range(1):
+            d_in.copy_(h_in, non_blocking=True)
+            step(d_in)
+            h_out.copy_(alm_out, non_blocking=True)
+        torch.cuda.synchronize()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(st)
+        for _ in range(a.steps):
+            d_in.copy_(h_in, non_blocking=True)
+            step(d_in)
+            h_out.copy_(alm_out, non_blocking=True)
+        f1.record(st)
+        torch.cuda.synchronize()
+        barrier()
+        ems = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([ems], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = alm_h.nbytes
+        e2e = {"value": world * a.nmaps * a.steps / (ems / 1e3), "unit": "maps/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "ms_per_step": ems / a.steps}
+
+    # ---------------- roofline of the dominant kernel ----------------
+    kms = {k: (kt["ms"][k] / kt["launches"][k] if kt["launches"][k] else 0.0) for k in kt["ms"]}
+    share = {k: kt["ms"][k] / max(sum(kt["ms"].values()), 1e-12) for k in kt["ms"]}
+    dominant = max(kt["ms"], key=lambda k: kt["ms"][k])
+    peak_hbm, hbm_src = measured_peaks()
+    if dominant.startswith("legendre"):
+        fp64 = fp64_peak_tflops(torch)
+        achieved = work["legendre_flops"] / (kms[dominant] / 1e3) / 1e12
+        roofline = {"bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": fp64,
+                    "unit": "TFLOP/s", "frac": achieved / fp64,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured by bench.py on this GPU "
+                                   "(FP64 is not in MEASURED_PEAKS.json)",
+                    "traffic": profile_traffic(dominant),
+                    "algorithmic_flops_per_launch": work["legendre_flops"],
+                    "matrix_bytes_per_launch": work["matrix_bytes"],
+                    "hbm_view": {"achieved_gbs": (work["matrix_bytes"] + work["legendre_vector_bytes"])
+                                 / (kms[dominant] / 1e3) / 1e9,
+                                 "peak_gbs": peak_hbm, "peak_source": hbm_src}}
+    else:
+        achieved = work["ring_bytes"] / (kms[dominant] / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_hbm,
+                    "unit": "GB/s", "frac": achieved / peak_hbm, "peak_source": hbm_src,
+                    "traffic": profile_traffic(dominant)}
+    roofline["kernel_ms_per_launch"] = kms
+    roofline["kernel_time_share"] = share
+
+    # ---------------- CPU baseline (rank 0, N = 1) ----------------
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            cpu = reference_rate(a, path, a.cpu_baseline_seconds)
+        except Exception as ex:  # reported, never fatal for the GPU number
+            cpu = {"value": None, "unit": "maps/s", "error": str(ex)[:200]}
+
+    launches = int(sum(kt["launches"].values()))
+    out = {
+        "metric": METRIC, "value": value, "unit": "maps/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1)(l+1)^-1 alm per map)",
+        "config": {"workload": "alm2map+map2alm round trip, nside %d, lmax=mmax %d, %d maps per GPU"
+                               % (a.nside, a.lmax, a.nmaps),
+                   "nside": a.nside, "lmax": a.lmax, "nmaps_per_gpu": a.nmaps,
+                   "precision": "plain FP64", "plan": {"eps": a.eps, "chunk": a.chunk,
+                                                       "memop_cost": a.memop},
+                   "parallelism": "replicas (maps sharded per GPU)" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (alm %.2f GB, maps %.2f GB per GPU)"
+                         % (alm_h.nbytes / 1e9, T.npix * a.nmaps * 8 / 1e9)},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk, "plan_work": work,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    T.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    path = ensure_plan(a, 0)
+    r = ReferenceRunner(a, path)
+    for _ in range(a.warmup):
+        r.execute()
+    times = [r.execute() for _ in range(a.steps)]
+    total = sum(times)
+    value = r.nmaps * len(times) / (2.0 * total)
+    cpu = {"value": value, "unit": "maps/s", "cores": r.threads, "kind": "reference",
+           "sample": r.describe(len(times))}
+    r.close()
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "maps/s",
+           "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": 1e3 * total / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded N(0,1)(l+1)^-1 alm)",
+           "config": {"workload": "alm2map+map2alm round trip, nside %d, lmax=mmax %d; each step "
+                                  "a sample of %d maps" % (a.nside, a.lmax, r.nmaps),
+                      "nside": a.nside, "lmax": a.lmax},
+           "cpu_baseline": cpu,
+           "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -45,8 +45,9 @@ wavemoth_plan wavemoth_plan_from_healpix(int Nside, int lmax, int mmax, int nmap
                                          double *input, double *output, int ordering,
                                          unsigned flags, char *resource_filename);
 
-/* Device-pointer execution on `stream` (a cudaStream_t; NULL = the plan's
-   own stream).  Asynchronous with respect to the host.  The plan's
+/* Device-pointer execution on `stream` (a cudaStream_t; NULL is the CUDA
+   default stream, as everywhere in the CUDA API).  Asynchronous with respect
+   to the host.  The plan's
    intermediate buffers are shared by all calls on one plan, so calls on one
    plan must not overlap in time (serialise them on one stream).
    alm: (nalm, nmaps) complex128 as interleaved doubles; map: (npix, nmaps). */
@@ -73,6 +74,20 @@ int64_t wavemoth_plan_program_bytes(wavemoth_plan plan);
    Plans whose buffers would exceed it fail with WAVEMOTH_ERR_NOMEM.  Used to
    exercise allocation-failure handling without exhausting the GPU. */
 void wavemoth_set_device_memory_cap(int64_t bytes);
+
+/* Per-kernel device timing of a plan, from CUDA events recorded on the
+   launching stream.  mode 1: reset and enable, 0: reset and disable,
+   2: read into out[8] = (ms Legendre alm2map, ms Legendre map2alm, ms ring
+   synthesis, ms ring analysis, and the four launch counts); reading waits
+   for the recorded events. */
+int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out);
+
+/* Algorithmic work of one transform direction of the plan for nmaps maps:
+   out[0] Legendre flops (2 per multiply-add, 5 per recurrence step),
+   out[1] compressed-matrix bytes read, out[2] alm + q bytes of one Legendre
+   launch, out[3] q + map bytes of one ring launch, out[4..6] interpolation /
+   recurrence / dense residual element counts, out[7] Legendre grid size. */
+int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out);
 
 /* Parses and validates a rev1 file for (Nside, lmax) exactly as plan
    creation does, without touching the GPU.  On success returns 0 and, if

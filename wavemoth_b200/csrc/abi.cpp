@@ -80,7 +80,13 @@ struct _wavemoth_plan {
   int64_t slot_stride = 0;
   cudaStream_t stream = nullptr;
 
+  // optional per-kernel event timing (wavemoth_plan_timing)
+  bool timing = false;
+  struct Span { int kind; cudaEvent_t a, b; };
+  std::vector<Span> spans;
+
   ~_wavemoth_plan() {
+    for (auto &s : spans) { cudaEventDestroy(s.a); cudaEventDestroy(s.b); }
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -287,6 +293,20 @@ wm::RingParams ring_params(wavemoth_plan P) {
   return r;
 }
 
+// kinds: 0 Legendre alm2map, 1 Legendre map2alm, 2 ring synthesis, 3 ring analysis
+int span_begin(wavemoth_plan P, int kind, cudaStream_t st) {
+  if (!P->timing) return -1;
+  _wavemoth_plan::Span s{kind, nullptr, nullptr};
+  if (cudaEventCreate(&s.a) != cudaSuccess || cudaEventCreate(&s.b) != cudaSuccess) return -1;
+  cudaEventRecord(s.a, st);
+  P->spans.push_back(s);
+  return (int)P->spans.size() - 1;
+}
+
+void span_end(wavemoth_plan P, int idx, cudaStream_t st) {
+  if (idx >= 0) cudaEventRecord(P->spans[idx].b, st);
+}
+
 int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_out,
                  const double *q_in, double *q_out, cudaStream_t st) {
   wm::LegendreParams p = legendre_params(P);
@@ -296,7 +316,10 @@ int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *al
   p.q_out = q_out;
   if (int rc = cuda_check(cudaMemsetAsync(P->d_counter, 0, sizeof(int32_t), st), "counter reset"))
     return rc;
-  return cuda_check(wm::launch_legendre(alm2map, p, P->grid, st), "Legendre kernel launch");
+  int sp = span_begin(P, alm2map ? 0 : 1, st);
+  int rc = cuda_check(wm::launch_legendre(alm2map, p, P->grid, st), "Legendre kernel launch");
+  span_end(P, sp, st);
+  return rc;
 }
 
 int run_alm2map(wavemoth_plan P, const double *alm, double *map, cudaStream_t st) {
@@ -304,14 +327,20 @@ int run_alm2map(wavemoth_plan P, const double *alm, double *map, cudaStream_t st
   wm::RingParams r = ring_params(P);
   r.q = P->d_q;
   r.map = map;
-  return cuda_check(wm::launch_ring_synthesis(r, st), "ring synthesis launch");
+  int sp = span_begin(P, 2, st);
+  int rc = cuda_check(wm::launch_ring_synthesis(r, st), "ring synthesis launch");
+  span_end(P, sp, st);
+  return rc;
 }
 
 int run_map2alm(wavemoth_plan P, const double *map, double *alm, cudaStream_t st) {
   wm::RingParams r = ring_params(P);
   r.map_in = map;
   r.q_out = P->d_q;
-  if (int rc = cuda_check(wm::launch_ring_analysis(r, st), "ring analysis launch")) return rc;
+  int sp = span_begin(P, 3, st);
+  int rc0 = cuda_check(wm::launch_ring_analysis(r, st), "ring analysis launch");
+  span_end(P, sp, st);
+  if (rc0) return rc0;
   return run_legendre(P, false, nullptr, alm, P->d_q, nullptr, st);
 }
 
@@ -417,15 +446,13 @@ int wavemoth_query_resourcefile(char *filename, int *out_Nside, int *out_lmax) {
 int wavemoth_execute_alm2map_device(wavemoth_plan plan, const double *alm, double *map,
                                     void *stream) {
   if (!plan || !alm || !map) return set_error(WAVEMOTH_ERR_ARG, "NULL plan or buffer");
-  cudaStream_t st = stream ? (cudaStream_t)stream : plan->stream;
-  return finish(plan, run_alm2map(plan, alm, map, st));
+  return finish(plan, run_alm2map(plan, alm, map, (cudaStream_t)stream));
 }
 
 int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, double *alm,
                                     void *stream) {
   if (!plan || !alm || !map) return set_error(WAVEMOTH_ERR_ARG, "NULL plan or buffer");
-  cudaStream_t st = stream ? (cudaStream_t)stream : plan->stream;
-  return finish(plan, run_map2alm(plan, map, alm, st));
+  return finish(plan, run_map2alm(plan, map, alm, (cudaStream_t)stream));
 }
 
 void wavemoth_perform_legendre_transforms(wavemoth_plan plan) {
@@ -487,6 +514,49 @@ int64_t wavemoth_plan_device_bytes(wavemoth_plan plan) { return plan ? plan->are
 int64_t wavemoth_plan_program_bytes(wavemoth_plan plan) { return plan ? plan->program_bytes : -1; }
 
 void wavemoth_set_device_memory_cap(int64_t bytes) { g_device_cap = bytes; }
+
+int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out) {
+  if (!plan) return set_error(WAVEMOTH_ERR_ARG, "NULL plan");
+  if (mode == 0 || mode == 1) {
+    if (plan->stream) cudaStreamSynchronize(plan->stream);
+    for (auto &s : plan->spans) { cudaEventDestroy(s.a); cudaEventDestroy(s.b); }
+    plan->spans.clear();
+    plan->timing = (mode == 1);
+    return 0;
+  }
+  if (mode != 2 || !out) return set_error(WAVEMOTH_ERR_ARG, "invalid timing mode");
+  for (int i = 0; i < 8; ++i) out[i] = 0.0;
+  for (auto &s : plan->spans) {
+    if (int rc = cuda_check(cudaEventSynchronize(s.b), "timing event")) return rc;
+    float ms = 0.f;
+    if (int rc = cuda_check(cudaEventElapsedTime(&ms, s.a, s.b), "timing event")) return rc;
+    out[s.kind] += ms;
+    out[4 + s.kind] += 1.0;
+  }
+  return 0;
+}
+
+int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out) {
+  if (!plan || !out || nmaps <= 0) return set_error(WAVEMOTH_ERR_ARG, "invalid arguments");
+  const auto &G = plan->prog;
+  const double nvecs = 2.0 * nmaps;
+  // Legendre: multiply-adds of the interpolation and residual products, plus
+  // 5 flops per recurrence element (shared by all vectors)
+  out[0] = 2.0 * nvecs * (double)(G.interp_elems + G.rec_elems + G.dense_elems) + 5.0 * (double)G.rec_elems;
+  // compressed-matrix bytes one direction streams: interpolants (one copy),
+  // dense residual values, x2/P0/P1 per recurrence column, coefficients
+  out[1] = 8.0 * (double)(G.interp_elems + G.dense_elems + 3 * G.rec_columns + G.aux_values);
+  // vector traffic of one Legendre launch: alm in (or out) and q out (or in)
+  const double nalm = (double)plan->nalm, nq = 2.0 * (plan->mmax + 1) * plan->ni;
+  out[2] = 8.0 * nvecs * (nalm + nq);
+  // ring kernels: q in (or out) and the maps out (or in)
+  out[3] = 8.0 * (nvecs * nq + (double)plan->npix * nmaps);
+  out[4] = (double)G.interp_elems;
+  out[5] = (double)G.rec_elems;
+  out[6] = (double)G.dense_elems;
+  out[7] = (double)plan->grid;
+  return 0;
+}
 
 int wavemoth_check_resourcefile(char *filename, int Nside, int lmax, int64_t *out_stats) {
   if (!filename) return set_error(WAVEMOTH_ERR_ARG, "NULL file name");

@@ -214,6 +214,7 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
           for (int c2 = 0; c2 < n - k; ++c2)
             for (int s2 = 0; s2 < k; ++s2) tr[c2 + (size_t)s2 * (n - k)] = ip[s2 + (size_t)c2 * k];
           size_t ipt = append_f64(P.f64, (const char *)tr.data(), nel);
+          P.interp_elems += (int64_t)nel;
           size_t mo = append_i32(P.i32, map), po = append_i32(P.i32, perm);
           if (j == 0) {
             pr.kT = k; pr.inT = offs[d][u][2 * i]; pr.mapT = mo; pr.permT = po;
@@ -295,6 +296,7 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
         if (!R.check(off, 8 * nel, "dense residual block")) return false;
         DevStrip S{0, 0, D.ncols, 0, (int32_t)P.dblocks.size(), 0,
                    (int64_t)append_f64(P.f64, R.base + off, nel)};
+        P.dense_elems += (int64_t)nel;
         P.strips.push_back(S);
         cost += (double)nel;
       } else {
@@ -306,6 +308,7 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
         size_t naux = 3 * (size_t)(nkb - 2);
         if (!R.check(off, 8 * naux, "recurrence coefficients")) return false;
         D.aux = (int64_t)append_f64(P.f64, R.base + off, naux);
+        P.aux_values += (int64_t)naux;
         off += 8 * naux;
         int32_t cstart = 0;
         for (int64_t s = 0; s < nstrips; ++s) {
@@ -322,6 +325,7 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
             if (!R.check(off, 8 * nel, "dense strip")) return false;
             S.data = (int64_t)append_f64(P.f64, R.base + off, nel);
             off += 8 * nel;
+            P.dense_elems += (int64_t)nel;
           } else {
             S.kind = 1;
             size_t o[3];
@@ -337,6 +341,8 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
             for (int a = 0; a < 3; ++a)
               memcpy(P.f64.data() + base + (size_t)a * nx, R.base + o[a], 8 * (size_t)nx);
             S.data = (int64_t)base;
+            P.rec_elems += (int64_t)nks * nx;
+            P.rec_columns += nx;
           }
           cost += (double)nks * nx * (S.kind ? 2.5 : 1.0);
           P.strips.push_back(S);

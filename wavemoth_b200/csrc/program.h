@@ -19,6 +19,12 @@ struct HostProgram {
   std::vector<double> f64;
   std::vector<int32_t> i32;
   std::vector<int64_t> element_count;   // header element_count per (2m + odd)
+  // algorithmic work of one transform direction
+  int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
+  int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)
+  int64_t dense_elems = 0;       // dense residual elements
+  int64_t rec_columns = 0;       // columns of recurrence strips (x2, P0, P1 each)
+  int64_t aux_values = 0;        // recurrence coefficients stored
 };
 
 // Parses a rev1 file image.  nside_expect < 0 accepts any nside.

@@ -18,7 +18,9 @@
 // per output from the table of roots).  All twiddles come from one table of
 // n-th roots of unity computed with sincospi on exact rationals.
 //
-// One CTA per (ring pair, map); ring lengths are 4, 8, ..., 4 nside.
+// One CTA per (map, ring pair), maps fastest in the grid so that the CTAs that
+// share the 32-byte sectors of q (16 bytes per map) and of the interleaved
+// (npix, nmaps) map run at the same time; ring lengths are 4, 8, ..., 4 nside.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -164,7 +166,7 @@ __device__ void build_roots(cplx *roots, int n) {
 __global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
   extern __shared__ double smem_d[];
   cplx *sm = reinterpret_cast<cplx *>(smem_d);
-  const int r = blockIdx.x, kmap = blockIdx.y;
+  const int kmap = blockIdx.x, r = blockIdx.y;
   const DevRing R = p.rings[r];
   const int n = R.n, N = n / 2;
   cplx *bufA = sm;
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
 __global__ void __launch_bounds__(kRingThreads) k_ring_analysis(RingParams p) {
   extern __shared__ double smem_d[];
   cplx *sm = reinterpret_cast<cplx *>(smem_d);
-  const int r = blockIdx.x, kmap = blockIdx.y;
+  const int kmap = blockIdx.x, r = blockIdx.y;
   const DevRing R = p.rings[r];
   const int n = R.n, N = n / 2;
   cplx *bufA = sm;
@@ -281,7 +283,7 @@ cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(k_ring_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(prm.ni, prm.nmaps);
+  dim3 grid(prm.nmaps, prm.ni);
   k_ring_synthesis<<<grid, kRingThreads, smem, st>>>(prm);
   return cudaGetLastError();
 }
@@ -291,7 +293,7 @@ cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(k_ring_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid(prm.ni, prm.nmaps);
+  dim3 grid(prm.nmaps, prm.ni);
   k_ring_analysis<<<grid, kRingThreads, smem, st>>>(prm);
   return cudaGetLastError();
 }

@@ -14,7 +14,10 @@ from .lib import WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WavemothError, last_
 
 
 class Transform:
-    def __init__(self, resource_file, nside, lmax, nmaps=1, directions=("alm2map", "map2alm")):
+    """Both directions share one device plan (the compiled butterfly program
+    serves A^T for alm2map and A for map2alm)."""
+
+    def __init__(self, resource_file, nside, lmax, nmaps=1):
         if not torch.cuda.is_available():
             raise RuntimeError("wavemoth_b200.Transform needs a CUDA device")
         self.nside, self.lmax, self.nmaps = nside, lmax, nmaps
@@ -22,14 +25,12 @@ class Transform:
         self.nalm = (lmax + 1) * (lmax + 2) // 2
         self.resource_file = resource_file
         lib = _native.lib()
-        self._plans = {}
-        for d in directions:
-            fn = lib.wavemoth_plan_to_healpix if d == "alm2map" else lib.wavemoth_plan_from_healpix
-            p = fn(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR,
-                   WAVEMOTH_DEVICE_POINTERS, os.fsencode(resource_file))
-            if not p:
-                raise WavemothError("plan creation failed: " + last_error())
-            self._plans[d] = p
+        p = lib.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR,
+                                         WAVEMOTH_DEVICE_POINTERS, os.fsencode(resource_file))
+        if not p:
+            raise WavemothError("plan creation failed: " + last_error())
+        self._plan = p
+        self._plans = {"alm2map": p, "map2alm": p}
 
     def _stream(self):
         return torch.cuda.current_stream().cuda_stream
@@ -66,9 +67,41 @@ class Transform:
             raise WavemothError("map2alm failed (%d): %s" % (rc, last_error()))
         return out
 
+    @property
+    def plan_handle(self):
+        return self._plan
+
+    def timing(self, mode):
+        """Per-kernel event timing: mode 1 enable/reset, 0 disable, 2 read
+        -> dict of milliseconds and launch counts."""
+        import ctypes
+        out = (ctypes.c_double * 8)()
+        rc = _native.lib().wavemoth_plan_timing(self._plan, mode, out)
+        if rc != 0:
+            raise WavemothError("timing failed: " + last_error())
+        if mode != 2:
+            return None
+        keys = ("legendre_alm2map", "legendre_map2alm", "ring_synthesis", "ring_analysis")
+        return {"ms": dict(zip(keys, list(out)[:4])), "launches": dict(zip(keys, list(out)[4:]))}
+
+    def work(self):
+        """Algorithmic work of one direction (see wavemoth_plan_work)."""
+        import ctypes
+        out = (ctypes.c_double * 8)()
+        rc = _native.lib().wavemoth_plan_work(self._plan, self.nmaps, out)
+        if rc != 0:
+            raise WavemothError("work query failed: " + last_error())
+        o = list(out)
+        return {"legendre_flops": o[0], "matrix_bytes": o[1], "legendre_vector_bytes": o[2],
+                "ring_bytes": o[3], "interp_elems": o[4], "rec_elems": o[5], "dense_elems": o[6],
+                "legendre_grid": o[7],
+                "device_bytes": _native.lib().wavemoth_plan_device_bytes(self._plan),
+                "program_bytes": _native.lib().wavemoth_plan_program_bytes(self._plan)}
+
     def close(self):
-        for p in self._plans.values():
-            _native.lib().wavemoth_destroy_plan(p)
+        if getattr(self, "_plan", None):
+            _native.lib().wavemoth_destroy_plan(self._plan)
+        self._plan = None
         self._plans = {}
 
     def __del__(self):
