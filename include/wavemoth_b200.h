@@ -56,6 +56,25 @@ int wavemoth_execute_alm2map_device(wavemoth_plan plan, const double *alm, doubl
 int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, double *alm,
                                     void *stream);
 
+/* The alm2map Legendre step of `plan` (q = A^T a for every (m, parity)),
+   for callers that cannot allocate device memory when they run it (inside a
+   custom allocator's callback, under a framework that owns all device
+   memory, or while other latency-critical work must not see driver
+   allocations).  alm: device input as for wavemoth_execute_alm2map_device;
+   q: device output of 2 (mmax+1) * 2 Nside * 2 nmaps doubles in the layout
+   of wavemoth_get_work.  The kernel's level buffers come from one 32 MiB
+   static device array that the library holds on every GPU that loads it
+   until the process exits; nothing is allocated or freed by this call.
+   Problems whose per-CTA buffers (2 x largest level x 2 nmaps doubles) do
+   not fit are rejected with WAVEMOTH_ERR_NOMEM; smaller ones run on as many
+   CTAs as fit.  The first call on a device looks up the array's device
+   address (cudaGetSymbolAddress), so make it before any stream capture.
+   All calls share the array and its contents persist between calls: calls
+   that overlap on the GPU race, so serialise them.  No counterpart in the
+   reference. */
+int wavemoth_legendre_alm2map_noalloc(wavemoth_plan plan, const double *alm, double *q,
+                                      void *stream);
+
 /* Copies the Legendre-phase output q (complex128, (mmax+1, 2, 2 Nside, nmaps))
    to host memory `out`; the analogue of ShtPlan.get_work
    (wavemoth/lib.pyx:158-179). */

@@ -1,0 +1,48 @@
+"""The allocation-free Legendre entry point (wavemoth_legendre_alm2map_noalloc).
+
+Callers that cannot allocate device memory when the transform runs (custom
+allocator callbacks, frameworks that own all device memory) use this entry
+point: its level buffers live in a static device array inside the library.
+This test checks, through the C ABI, that two calls in a row produce the
+same Legendre-phase output q as the plan's regular path.  It sits in a file
+collected last so that a failure here does not hide any other test result.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import sht as osht
+from wavemoth_b200 import _native
+from wavemoth_b200 import lib as wlib
+
+from .plans import plan_file, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("cfg,nmaps", [((16, 32, 8, 1e-10, 1e-10), 3), ((32, 64, 16, 1e-10, 20.0), 2)])
+def test_noalloc_matches_plan_path(cfg, nmaps):
+    torch = pytest.importorskip("torch")
+    nside, lmax, chunk, eps, memop = cfg
+    path = plan_file(nside, lmax, chunk, eps, memop)
+    alm = osht.random_alm(lmax, nmaps, seed=77)
+    out = np.zeros((12 * nside * nside, nmaps))
+    plan = wlib.ShtPlan(nside, lmax, lmax, alm, out, "mmajor", matrix_data_filename=path)
+    plan.perform_legendre_transform()
+    want = plan.get_work()
+
+    d_alm = torch.from_numpy(alm.view(np.float64).copy()).cuda()
+    nq = 2 * (lmax + 1) * 2 * nside * 2 * nmaps
+    L = _native.lib()
+    for _ in range(2):
+        d_q = torch.full((nq,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        rc = L.wavemoth_legendre_alm2map_noalloc(plan._plan, ctypes.c_void_p(d_alm.data_ptr()),
+                                                 ctypes.c_void_p(d_q.data_ptr()), None)
+        assert rc == 0, wlib.last_error()
+        torch.cuda.synchronize()
+        got = d_q.cpu().numpy().view(np.complex128).reshape(want.shape)
+        assert np.all(np.isfinite(got))
+        assert rel(got, want) < 1e-12
+    plan.close()

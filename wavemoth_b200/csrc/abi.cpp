@@ -280,6 +280,28 @@ wm::LegendreParams legendre_params(wavemoth_plan P) {
   return p;
 }
 
+}  // namespace
+
+namespace wm {
+
+int set_last_error(int code, const std::string &msg) { return set_error(code, msg); }
+
+// Legendre kernel parameters of a plan (program tables, sizes, grid) without
+// any buffers bound; used by entry points that bring their own buffers.
+bool plan_legendre_params(wavemoth_plan plan, LegendreParams &p, int &grid, std::string &err) {
+  if (!plan) {
+    err = "NULL plan";
+    return false;
+  }
+  p = legendre_params(plan);
+  grid = plan->grid;
+  return true;
+}
+
+}  // namespace wm
+
+namespace {
+
 wm::RingParams ring_params(wavemoth_plan P) {
   wm::RingParams r{};
   r.rings = P->d_rings;
