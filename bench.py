@@ -104,6 +104,26 @@ def synthetic_alm(lmax, nmaps, seed0, power=1.0):
     return out
 
 
+def rank_seed(rank, nmaps):
+    """First generator seed of a rank's batch: the ranks' maps are disjoint."""
+    return 1000 + rank * nmaps
+
+
+def reduce_max_seconds(t, dist=None, device="cuda"):
+    """Slowest rank's time (the job's time)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return t
+    import torch
+    x = torch.tensor([t], dtype=torch.float64, device=device)
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return float(x.item())
+
+
+def job_rate(world, nmaps, steps, seconds):
+    """Whole-job maps per second: every rank's maps over the slowest time."""
+    return world * nmaps * steps / seconds
+
+
 # ------------------------------------------------------------------- clocks
 
 class ClockSampler:
@@ -268,7 +288,7 @@ def run_b200(a):
     T = Transform(path, a.nside, a.lmax, a.nmaps)
     log("plan loaded in %.1f s" % (time.time() - t0))
     work = T.work()
-    alm_h = synthetic_alm(a.lmax, a.nmaps, 1000 + rank * a.nmaps)
+    alm_h = synthetic_alm(a.lmax, a.nmaps, rank_seed(rank, a.nmaps))
     alm = torch.from_numpy(alm_h).cuda()
     maps = torch.empty((T.npix, a.nmaps), dtype=torch.float64, device="cuda")
     alm_out = torch.empty_like(alm)
@@ -298,12 +318,9 @@ def run_b200(a):
     ms = e0.elapsed_time(e1)
     kt = T.timing(2)
     T.timing(0)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = 1e3 * reduce_max_seconds(ms / 1e3, dist if world > 1 else None)
     ms_per_step = ms / a.steps
-    value = world * a.nmaps * a.steps / (ms / 1e3)
+    value = job_rate(world, a.nmaps, a.steps, ms / 1e3)
 
     # ---------------- end to end (host buffers) ----------------
     e2e = None
@@ -327,13 +344,9 @@ def run_b200(a):
         f1.record(st)
         torch.cuda.synchronize()
         barrier()
-        ems = f0.elapsed_time(f1)
-        if world > 1:
-            t = torch.tensor([ems], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = 1e3 * reduce_max_seconds(f0.elapsed_time(f1) / 1e3, dist if world > 1 else None)
         nbytes = alm_h.nbytes
-        e2e = {"value": world * a.nmaps * a.steps / (ems / 1e3), "unit": "maps/s",
+        e2e = {"value": job_rate(world, a.nmaps, a.steps, ems / 1e3), "unit": "maps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "ms_per_step": ems / a.steps}
 

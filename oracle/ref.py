@@ -101,6 +101,59 @@ def query_resourcefile(path):
     return rc, n.value, l.value
 
 
+PULL_FUNC = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t,
+                             ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                             ctypes.c_void_p)
+
+
+def bfm_transpose_apply(matrix_bytes, x, mode="rows"):
+    """The reference's own bfm_transpose_apply_d (src/butterfly.c.in:375-432)
+    on a serialized matrix, with the pull callbacks of its Python test
+    harness: mode "rows" copies input rows (ButterflyPlan,
+    butterfly.pyx:134-141), mode "dense" applies a dense residual payload
+    (DenseResidualButterfly, butterfly.pyx:144-161)."""
+    import struct
+    L = lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    nvecs = x.shape[1]
+    raw = np.zeros(len(matrix_bytes) + 32, np.uint8)
+    off = (-raw.ctypes.data) % 16
+    buf = raw[off:off + len(matrix_bytes)]
+    buf[:] = np.frombuffer(matrix_bytes, np.uint8)
+    nrows, ncols, k_max, nblocks_max = struct.unpack_from("<iiii", matrix_bytes, 0)
+    sems = (ctypes.c_char * 64)()
+    L.bfm_create_plan.restype = ctypes.c_void_p
+    L.bfm_create_plan.argtypes = [ctypes.c_size_t] * 3 + [ctypes.c_void_p] * 2
+    L.bfm_transpose_apply_d.restype = ctypes.c_int
+    L.bfm_transpose_apply_d.argtypes = [ctypes.c_void_p, ctypes.c_void_p, PULL_FUNC,
+                                        ctypes.POINTER(ctypes.c_double), ctypes.c_size_t,
+                                        ctypes.c_void_p]
+    plan = L.bfm_create_plan(max(k_max, max(nrows, 1)), max(nblocks_max, 1), nvecs,
+                             ctypes.addressof(sems), ctypes.addressof(sems) + 32)
+    out = np.zeros((ncols, nvecs))
+
+    def pull(bufp, start, stop, nv, payload, plen, ctx):
+        n = stop - start
+        dst = np.ctypeslib.as_array(bufp, shape=(max(n, 1) * nv,))[:n * nv].reshape(n, nv) if n else None
+        if mode == "rows":
+            if n:
+                dst[:] = x[start:stop]
+            return
+        p = payload + ((-payload) % 16)
+        rs, re = struct.unpack("<qq", ctypes.string_at(p, 16))
+        k = re - rs
+        if n:
+            A = np.frombuffer(ctypes.string_at(p + 16, 8 * k * n), np.float64).reshape((k, n), order="F")
+            dst[:] = A.T @ x[rs:re]
+
+    cb = PULL_FUNC(pull)
+    rc = L.bfm_transpose_apply_d(plan, buf.ctypes.data, cb,
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size, None)
+    if rc != 0:
+        raise RuntimeError("bfm_transpose_apply_d: %d" % rc)
+    return out
+
+
 class RefPlan:
     def __init__(self, nside, lmax, nmaps, resource_file, nthreads=1, phase_shifts=True,
                  attempts=50):

@@ -282,6 +282,29 @@ class Matrix:
         assert start == self.ncols
         return q
 
+    def transpose_apply_rows(self, x):
+        """y = A^T x where the residual factor is the identity: root block j
+        takes rows [pos, pos + k_j) of x in order (the pull of
+        ButterflyPlan.transpose_pull_input, butterfly.pyx:134-141)."""
+        nvecs = x.shape[1]
+        q = np.zeros((self.ncols, nvecs))
+        start = 0
+        pos_in = 0
+        for r in range(self.first_level_size):
+            pos = self.heap_first_index + r
+            nb, bh, _ = self.node(pos)
+            if nb == 0:
+                q[start:start + bh[0]] = x[pos_in:pos_in + bh[0]]
+                pos_in += bh[0]
+                start += bh[0]
+            else:
+                inputs = []
+                for j in range(nb):
+                    inputs.append(x[pos_in:pos_in + bh[j]])
+                    pos_in += bh[j]
+                start = self._t_node(pos, start, inputs, q)
+        return q
+
     def _t_node(self, pos, start, inputs, q):
         nb, bh, _ = self.node(pos)
         if nb == 0:

@@ -153,7 +153,7 @@ class IdentityNode:
 
 
 class InnerNode:
-    def __init__(self, blocks, children, remainder_blocks):
+    def __init__(self, blocks, children, remainder_blocks=None):
         L, R = children
         for (T, B), lh, rh in zip(blocks, L.block_heights, R.block_heights):
             if not (T.n == B.n == lh + rh):
@@ -164,8 +164,16 @@ class InnerNode:
         self.node_ncols = L.node_nrows + R.node_nrows
         self.block_heights = [h for T, B in blocks for h in (T.k, B.k)]
         self.node_nrows = sum(self.block_heights)
+        if remainder_blocks is None:
+            # a bare interpolation node (butterfly.pyx:326-329)
+            remainder_blocks = [ResidualBlock(0, h, np.zeros(0, np.int64))
+                                for h in self.block_heights]
+            self.nrows = self.node_nrows
+        else:
+            if len(remainder_blocks) != len(self.block_heights):
+                raise ValueError("remainder_blocks has wrong length")
+            self.nrows = sum(r.row_stop - r.row_start for r in remainder_blocks)
         self.remainder_blocks = remainder_blocks
-        self.nrows = sum(r.row_stop - r.row_start for r in remainder_blocks)
 
     def get_max_depth(self):
         return 1 + max(c.get_max_depth() for c in self.children)
@@ -255,8 +263,15 @@ def sparse_interpolative_decomposition(A, eps):
     return iden, ipol, proj
 
 
-def butterfly_compress(provider, chunk_size, shape, eps=1e-10):
-    """Butterfly tree of the (nrows, ncols) matrix served by provider.get_block."""
+def butterfly_compress(provider, chunk_size, shape=None, eps=1e-10):
+    """Butterfly tree of the (nrows, ncols) matrix served by provider.get_block
+    (an ndarray is wrapped in an ArrayProvider)."""
+    if isinstance(provider, np.ndarray):
+        if shape is None:
+            shape = provider.shape
+        provider = ArrayProvider(provider)
+    elif shape is None:
+        raise TypeError("shape must be provided")
     nrows, ncols = shape
     partition = pad_with_empty_columns(make_partition(0, ncols, chunk_size))
 
@@ -394,6 +409,25 @@ def serialize_butterfly_matrix(root, provider, num_levels=None, stream=None):
         _i64(stream, o - start)
     stream.seek(end)
     return stream
+
+
+class ArrayProvider:
+    """Serves blocks of an in-memory matrix; payloads are dense column-major
+    blocks (butterfly.pyx:642-658)."""
+
+    def __init__(self, array):
+        self.array = np.asarray(array, dtype=np.float64)
+
+    def get_block(self, row_start, row_stop, col_indices):
+        if len(col_indices) > 0:
+            return self.array[row_start:row_stop][:, col_indices]
+        return np.zeros((row_stop - row_start, 0))
+
+    def serialize_block_payload(self, stream, row_start, row_stop, col_indices):
+        _pad16(stream)
+        _i64(stream, row_start)
+        _i64(stream, row_stop)
+        _raw(stream, self.get_block(row_start, row_stop, col_indices), order="F")
 
 
 # --------------------------------------------------------------------------
