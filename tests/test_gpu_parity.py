@@ -51,6 +51,28 @@ def _map2alm_gpu(path, nside, lmax, maps):
 @pytest.mark.parametrize("cfg", CONFIGS)
 @pytest.mark.parametrize("nmaps", [1, 3])
 def test_alm2map_matches_oracle(cfg, nmaps):
+    _alm2map_case(cfg, nmaps)
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[3]])
+@pytest.mark.parametrize("nmaps", [5, 17, 40])
+def test_alm2map_many_maps(cfg, nmaps):
+    """Vector blocking of the tensor-core path: 10, 34 and 80 real vectors."""
+    _alm2map_case(cfg, nmaps)
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[3]])
+@pytest.mark.parametrize("nmaps", [5, 40])
+def test_map2alm_many_maps(cfg, nmaps):
+    nside, lmax, chunk, eps, memop = cfg
+    path = plan_file(nside, lmax, chunk, eps, memop)
+    maps = np.random.default_rng(nmaps).standard_normal((12 * nside * nside, nmaps))
+    got = _map2alm_gpu(path, nside, lmax, maps)
+    want = osht.map2alm_butterfly(osht.Rev1File(path), maps, lmax)
+    assert rel(got, want) < 1e-10
+
+
+def _alm2map_case(cfg, nmaps):
     nside, lmax, chunk, eps, memop = cfg
     path = plan_file(nside, lmax, chunk, eps, memop)
     alm = osht.random_alm(lmax, nmaps, seed=100 + nmaps)

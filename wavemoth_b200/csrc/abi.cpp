@@ -73,8 +73,18 @@ struct _wavemoth_plan {
   wm::DevPair *d_pairs = nullptr;
   double *d_f64 = nullptr;
   int32_t *d_i32 = nullptr;
-  int32_t *d_order = nullptr;
+  int32_t *d_order = nullptr;       // all matrices, largest first (generic kernel over everything)
+  int32_t *d_order_slow = nullptr;  // matrices left to the generic kernel by the tensor-core path
+  int32_t nslow = 0;
   int32_t *d_counter = nullptr;
+  // tensor-core path
+  wm::DevGroup *d_groups = nullptr;
+  wm::DevGCol *d_gcols = nullptr;
+  wm::DevTileA *d_tiles_a = nullptr;
+  wm::DevTileB *d_tiles_b = nullptr;
+  wm::DevRootUnit *d_roots = nullptr;
+  double *d_seeds = nullptr;
+  double *d_xbuf = nullptr;
   wm::DevRing *d_rings = nullptr;
   double *d_alm = nullptr, *d_map = nullptr, *d_q = nullptr, *d_scratch = nullptr;
   int64_t slot_stride = 0;
@@ -166,6 +176,33 @@ std::vector<wm::DevRing> ring_table(int nside) {
   return out;
 }
 
+wm::FastParams fast_params(wavemoth_plan P) {
+  const auto &G = P->prog;
+  wm::FastParams f{};
+  f.mats = P->d_mats;
+  f.pairs = P->d_pairs;
+  f.f64 = P->d_f64;
+  f.i32 = P->d_i32;
+  f.groups = P->d_groups;
+  f.gcols = P->d_gcols;
+  f.tiles_a = P->d_tiles_a;
+  f.tiles_b = P->d_tiles_b;
+  f.roots = P->d_roots;
+  f.seeds = P->d_seeds;
+  f.ngroups = (int32_t)G.groups.size();
+  f.ngcols = (int64_t)G.gcols.size();
+  f.ntiles_a = (int32_t)G.tiles_a.size();
+  f.ntiles_b = (int32_t)G.tiles_b.size();
+  f.nroots = (int32_t)G.roots.size();
+  f.max_root_k = G.max_root_k;
+  f.max_root_n = G.max_root_n;
+  f.lmax = P->lmax;
+  f.nvecs = P->nvecs;
+  f.ni = P->ni;
+  f.xbuf = P->d_xbuf;
+  return f;
+}
+
 wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps, double *input,
                         double *output, int ordering, unsigned flags, const char *resource_filename) {
   if (nmaps <= 0 || lmax < 0 || mmax != lmax || ordering != WAVEMOTH_MMAJOR) {
@@ -218,6 +255,11 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
     return nullptr;
   }
   auto &G = P->prog;
+  if (!wm::build_fast_path(G, err)) {
+    set_error(WAVEMOTH_ERR_RESOURCE, path + ": " + err);
+    delete P;
+    return nullptr;
+  }
   // processing order: largest matrices first
   std::vector<int32_t> order(G.mats.size());
   std::iota(order.begin(), order.end(), 0);
@@ -236,7 +278,23 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   rc = rc ? rc : upload(A, &P->d_f64, G.f64, "f64 arena");
   rc = rc ? rc : upload(A, &P->d_i32, G.i32, "i32 arena");
   rc = rc ? rc : upload(A, &P->d_order, order, "order");
+  {
+    std::vector<int32_t> slow;
+    std::vector<char> is_slow(G.mats.size(), 0);
+    for (int32_t mi : G.slow_mats) is_slow[mi] = 1;
+    for (int32_t mi : order)
+      if (is_slow[mi]) slow.push_back(mi);
+    P->nslow = (int32_t)slow.size();
+    rc = rc ? rc : upload(A, &P->d_order_slow, slow, "slow order");
+  }
+  rc = rc ? rc : upload(A, &P->d_groups, G.groups, "groups");
+  rc = rc ? rc : upload(A, &P->d_gcols, G.gcols, "group columns");
+  rc = rc ? rc : upload(A, &P->d_tiles_a, G.tiles_a, "alm2map tiles");
+  rc = rc ? rc : upload(A, &P->d_tiles_b, G.tiles_b, "map2alm tiles");
+  rc = rc ? rc : upload(A, &P->d_roots, G.roots, "roots");
+  rc = rc ? rc : A.alloc(&P->d_seeds, (size_t)std::max<int64_t>(G.nseeds, 1), "recurrence seeds");
   P->program_bytes = A.bytes;
+  rc = rc ? rc : A.alloc(&P->d_xbuf, (size_t)std::max<int64_t>(G.xrows, 1) * P->nvecs, "X buffer");
   rc = rc ? rc : upload(A, &P->d_rings, ring_table(P->nside), "ring table");
   rc = rc ? rc : A.alloc(&P->d_counter, 1, "counter");
   rc = rc ? rc : A.alloc(&P->d_q, (size_t)2 * (mmax + 1) * P->ni * P->nvecs, "q buffer");
@@ -247,6 +305,12 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   }
   rc = rc ? rc : cuda_check(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking),
                             "cudaStreamCreate");
+  if (!rc && G.nseeds > 0) {
+    wm::FastParams fp = fast_params(P);
+    fp.seeds_out = P->d_seeds;
+    rc = cuda_check(wm::launch_seeds(fp, P->stream), "seed kernel launch");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "seed kernel");
+  }
   if (rc) {
     delete P;
     return nullptr;
@@ -257,6 +321,8 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   G.pairs.clear(); G.pairs.shrink_to_fit();
   G.f64.clear(); G.f64.shrink_to_fit();
   G.i32.clear(); G.i32.shrink_to_fit();
+  G.gcols.clear(); G.gcols.shrink_to_fit();
+  G.tiles_a.shrink_to_fit();
   return P;
 }
 
@@ -329,17 +395,41 @@ void span_end(wavemoth_plan P, int idx, cudaStream_t st) {
   if (idx >= 0) cudaEventRecord(P->spans[idx].b, st);
 }
 
+int fast_grid(wavemoth_plan P, int units) {
+  return std::max(1, std::min(units, 4 * P->sm_count));
+}
+
 int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_out,
                  const double *q_in, double *q_out, cudaStream_t st) {
-  wm::LegendreParams p = legendre_params(P);
-  p.alm_in = alm_in;
-  p.alm_out = alm_out;
-  p.q_in = q_in;
-  p.q_out = q_out;
-  if (int rc = cuda_check(cudaMemsetAsync(P->d_counter, 0, sizeof(int32_t), st), "counter reset"))
-    return rc;
+  const auto &G = P->prog;
   int sp = span_begin(P, alm2map ? 0 : 1, st);
-  int rc = cuda_check(wm::launch_legendre(alm2map, p, P->grid, st), "Legendre kernel launch");
+  int rc = 0;
+  wm::FastParams f = fast_params(P);
+  f.alm_in = alm_in;
+  f.alm_out = alm_out;
+  f.q_in = q_in;
+  f.q = q_out;
+  const int nta = (int)G.tiles_a.size(), ntb = (int)G.tiles_b.size(), nr = (int)G.roots.size();
+  if (alm2map) {
+    if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
+    if (!rc && nr) rc = cuda_check(wm::launch_fast(1, f, fast_grid(P, nr), st), "alm2map level launch");
+  } else {
+    if (nr) rc = cuda_check(wm::launch_fast(2, f, fast_grid(P, nr), st), "map2alm level launch");
+    if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
+  }
+  if (!rc && P->nslow > 0) {
+    wm::LegendreParams p = legendre_params(P);
+    p.order = P->d_order_slow;
+    p.nmats = P->nslow;
+    p.alm_in = alm_in;
+    p.alm_out = alm_out;
+    p.q_in = q_in;
+    p.q_out = q_out;
+    rc = cuda_check(cudaMemsetAsync(P->d_counter, 0, sizeof(int32_t), st), "counter reset");
+    if (!rc)
+      rc = cuda_check(wm::launch_legendre(alm2map, p, std::min(P->grid, std::max(1, (int)P->nslow)), st),
+                      "Legendre kernel launch");
+  }
   span_end(P, sp, st);
   return rc;
 }
@@ -587,6 +677,8 @@ int wavemoth_check_resourcefile(char *filename, int Nside, int lmax, int64_t *ou
   if (!read_file(filename, file, err)) return set_error(WAVEMOTH_ERR_RESOURCE, err);
   wm::HostProgram P;
   if (!wm::compile_resource(file.data(), file.size(), Nside, lmax, lmax, P, err))
+    return set_error(WAVEMOTH_ERR_RESOURCE, std::string(filename) + ": " + err);
+  if (!wm::build_fast_path(P, err))
     return set_error(WAVEMOTH_ERR_RESOURCE, std::string(filename) + ": " + err);
   if (out_stats) {
     out_stats[0] = (int64_t)P.mats.size();

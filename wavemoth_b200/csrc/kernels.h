@@ -29,6 +29,35 @@ struct LegendreParams {
   int32_t *counter;       // work queue head (zeroed before launch)
 };
 
+struct FastParams {
+  const DevMatrix *mats;
+  const DevPair *pairs;
+  const double *f64;
+  const int32_t *i32;
+  const DevGroup *groups;
+  const DevGCol *gcols;
+  const DevTileA *tiles_a;
+  const DevTileB *tiles_b;
+  const DevRootUnit *roots;
+  const double *seeds;     // read by the map2alm residual kernel
+  double *seeds_out;       // written by the seed kernel (plan creation)
+  int32_t ngroups;
+  int64_t ngcols;
+  int32_t ntiles_a, ntiles_b, nroots;
+  int32_t max_root_k, max_root_n;
+  int32_t lmax, nvecs, ni;
+  const double *alm_in;    // alm2map input
+  double *alm_out;         // map2alm output
+  const double *q_in;      // map2alm input q~
+  double *q;               // alm2map output q
+  double *xbuf;            // depth-1 root blocks: X buffer (xrows x nvecs)
+};
+
+// which: 0 alm2map residual, 1 alm2map level, 2 map2alm level, 3 map2alm residual
+cudaError_t launch_fast(int which, const FastParams &prm, int grid, cudaStream_t st);
+cudaError_t launch_seeds(const FastParams &prm, cudaStream_t st);
+int fast_vector_tiles(int nvecs);
+
 int legendre_threads();
 cudaError_t launch_legendre(bool alm2map, const LegendreParams &prm, int grid, cudaStream_t st);
 

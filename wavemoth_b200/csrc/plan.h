@@ -71,7 +71,53 @@ struct DevMatrix {
   int32_t max_rows;      // rows of the largest intermediate buffer
   int64_t root_map;      // i32 arena, 2 per depth-0 row: (strip index, column within the strip)
   double cost;           // estimated work, for scheduling
+  int64_t xrow;          // first row of this matrix in the X buffer (depth-1 matrices), else -1
+  int32_t fast;          // 1: handled by the tensor-core path (depth <= 1)
+  int32_t pad2;
 };
+
+// ---- tensor-core (DMMA) path for matrices of tree depth 0 or 1 ----
+//
+// A "row group" is the set of residual blocks that share one range of matrix
+// rows: the single block of a depth-0 matrix, or the T (respectively B)
+// blocks of all roots of a depth-1 matrix.  The residual products of a group
+// are one GEMM with K = rows (alm2map) or K = the group's skeleton columns
+// (map2alm) and a recurrence-generated operand.
+struct DevGroup {
+  int32_t matrix;     // index into the matrix table
+  int32_t rs;         // first matrix row of the group
+  int32_t nrows;
+  int32_t ncols;      // skeleton columns of all the group's blocks
+  int64_t cols;       // index of the group's first DevGCol
+  int64_t seeds;      // index (in doubles) of the group's seeds: ncols x nchunks x 2
+  int32_t nchunks;    // row chunks of kPushRows rows
+  int32_t in_q;       // 1: the columns are rows of q (depth 0); 0: rows of the X buffer
+};
+
+struct DevGCol {
+  int32_t row;        // row of this column in q or in the matrix's X buffer
+  int32_t start;      // first active row (group coordinates); rows before it are zero
+  int32_t boff;       // residual-block row offset: block row = group row - boff
+  int32_t kind;       // 0: dense column, 1: recurrence
+  int64_t data;       // dense: f64 offset of row `start`; recurrence: f64 offset of x^2
+  int32_t nx;         // recurrence: stride from x^2 to P0 to P1
+  int32_t pad;
+  int64_t aux;        // f64 offset of the block's recurrence coefficients
+};
+
+struct DevTileA {     // alm2map residual unit: <= 64 consecutive group columns
+  int32_t group, col0, ncols, kstart;
+};
+
+struct DevTileB {     // map2alm residual unit: <= kPushRows consecutive group rows
+  int32_t group, row0, nrows, chunk;
+};
+
+struct DevRootUnit {  // depth-1 level unit: one root's interpolation pair
+  int32_t matrix, pair;
+};
+
+constexpr int kPushRows = 32;
 
 // Per ring pair (ring number r from the equator).
 struct DevRing {

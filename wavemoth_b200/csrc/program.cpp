@@ -438,3 +438,122 @@ bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_e
 }
 
 }  // namespace wm
+
+namespace wm {
+
+// Row groups, column tables, work units and seed bookkeeping of the
+// tensor-core path (plan.h).  Matrices of depth 0 (one residual block over
+// all rows) and depth 1 (every root a (T, B) pair over two leaves, T blocks
+// on rows [0, nk/2), B blocks on [nk/2, nk) -- butterfly.pyx:570-573) are
+// taken; anything else stays with the generic kernels.
+bool build_fast_path(HostProgram &P, std::string &err) {
+  P.groups.clear();
+  P.gcols.clear();
+  P.tiles_a.clear();
+  P.tiles_b.clear();
+  P.roots.clear();
+  P.slow_mats.clear();
+  P.nseeds = 0;
+  P.xrows = 0;
+  P.max_root_k = 0;
+  P.max_root_n = 0;
+  for (size_t mi = 0; mi < P.mats.size(); ++mi) {
+    DevMatrix &M = P.mats[mi];
+    M.fast = 0;
+    M.xrow = -1;
+    const int nblk = M.dblock_end - M.dblock_begin;
+    bool ok = M.nk > 0 && (M.nlevels == 0 || M.nlevels == 1);
+    if (ok && M.nlevels == 0) ok = (nblk == 1);
+    if (ok && M.nlevels == 1) {
+      ok = (nblk % 2 == 0);
+      const DevLevel &L = P.levels[M.level_begin];
+      ok = ok && (L.pair_end - L.pair_begin) * 2 == nblk;
+    }
+    // row ranges of the groups
+    std::vector<std::pair<int32_t, int32_t>> ranges;
+    if (ok) {
+      if (M.nlevels == 0) ranges = {{0, M.nk}};
+      else ranges = {{0, M.nk / 2}, {M.nk / 2, M.nk}};
+      for (int b = 0; b < nblk && ok; ++b) {
+        const DevDBlock &D = P.dblocks[M.dblock_begin + b];
+        const auto &rg = ranges[M.nlevels == 0 ? 0 : (b % 2)];
+        if (D.nrows == 0) continue;
+        ok = D.row_start >= rg.first && D.row_start + D.nrows == rg.second;
+      }
+    }
+    if (!ok) {
+      P.slow_mats.push_back((int32_t)mi);
+      continue;
+    }
+    M.fast = 1;
+    if (M.nlevels == 1) {
+      M.xrow = P.xrows;
+      P.xrows += M.root_rows;
+      const DevLevel &L = P.levels[M.level_begin];
+      for (int32_t pi = L.pair_begin; pi < L.pair_end; ++pi) {
+        const DevPair &pr = P.pairs[pi];
+        if (pr.out_right != pr.out_left + pr.n_left) {
+          err = "depth-1 root whose leaves are not adjacent";
+          return false;
+        }
+        P.roots.push_back(DevRootUnit{(int32_t)mi, pi});
+        P.max_root_k = std::max(P.max_root_k, pr.kT + pr.kB);
+        P.max_root_n = std::max(P.max_root_n, pr.n);
+      }
+    }
+    for (size_t g = 0; g < ranges.size(); ++g) {
+      DevGroup G{};
+      G.matrix = (int32_t)mi;
+      G.rs = ranges[g].first;
+      G.nrows = ranges[g].second - ranges[g].first;
+      G.cols = (int64_t)P.gcols.size();
+      G.in_q = M.nlevels == 0 ? 1 : 0;
+      for (int b = 0; b < nblk; ++b) {
+        if (M.nlevels == 1 && (size_t)(b % 2) != g) continue;
+        const DevDBlock &D = P.dblocks[M.dblock_begin + b];
+        const int32_t boff = D.nrows ? D.row_start - G.rs : G.nrows;
+        for (int32_t c = 0; c < D.ncols; ++c) {
+          DevGCol C{};
+          C.row = D.out_row + c;
+          C.boff = boff;
+          C.aux = D.aux;
+          C.start = G.nrows;  // inactive unless a strip covers it
+          for (int32_t s = D.strip_begin; s < D.strip_end; ++s) {
+            const DevStrip &S = P.strips[s];
+            if (c < S.cstart || c >= S.cstop) continue;
+            const int32_t nks = D.nrows - S.rstart;
+            if (D.nrows == 0 || nks <= 0) break;
+            C.start = boff + S.rstart;
+            C.kind = S.kind;
+            if (S.kind == 0) {
+              C.data = S.data + (int64_t)(c - S.cstart) * nks;
+            } else {
+              C.nx = S.cstop - S.cstart;
+              C.data = S.data + (c - S.cstart);
+            }
+            break;
+          }
+          P.gcols.push_back(C);
+        }
+      }
+      G.ncols = (int32_t)(P.gcols.size() - G.cols);
+      G.nchunks = (G.nrows + kPushRows - 1) / kPushRows;
+      G.seeds = P.nseeds;
+      P.nseeds += 2LL * G.ncols * G.nchunks;
+      const int32_t gi = (int32_t)P.groups.size();
+      P.groups.push_back(G);
+      for (int32_t c0 = 0; c0 < G.ncols; c0 += 64) {
+        DevTileA T{gi, c0, std::min(64, G.ncols - c0), G.nrows};
+        for (int32_t c = c0; c < c0 + T.ncols; ++c)
+          T.kstart = std::min(T.kstart, P.gcols[G.cols + c].start);
+        T.kstart &= ~3;
+        P.tiles_a.push_back(T);
+      }
+      for (int32_t j = 0; j < G.nchunks; ++j)
+        P.tiles_b.push_back(DevTileB{gi, j * kPushRows, std::min(kPushRows, G.nrows - j * kPushRows), j});
+    }
+  }
+  return true;
+}
+
+}  // namespace wm

@@ -19,6 +19,17 @@ struct HostProgram {
   std::vector<double> f64;
   std::vector<int32_t> i32;
   std::vector<int64_t> element_count;   // header element_count per (2m + odd)
+  // tensor-core path tables (see plan.h)
+  std::vector<DevGroup> groups;
+  std::vector<DevGCol> gcols;
+  std::vector<DevTileA> tiles_a;
+  std::vector<DevTileB> tiles_b;
+  std::vector<DevRootUnit> roots;
+  std::vector<int32_t> slow_mats;       // matrices left to the generic kernels
+  int64_t nseeds = 0;                   // doubles of recurrence seeds
+  int64_t xrows = 0;                    // rows of the X buffer
+  int32_t max_root_k = 0;               // largest kT + kB of a depth-1 root
+  int32_t max_root_n = 0;               // largest n of a depth-1 root
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)
@@ -26,6 +37,9 @@ struct HostProgram {
   int64_t rec_columns = 0;       // columns of recurrence strips (x2, P0, P1 each)
   int64_t aux_values = 0;        // recurrence coefficients stored
 };
+
+// Builds the tensor-core path tables for matrices of depth 0 and 1.
+bool build_fast_path(HostProgram &P, std::string &err);
 
 // Parses a rev1 file image.  nside_expect < 0 accepts any nside.
 bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_expect,
