@@ -86,6 +86,8 @@ struct _wavemoth_plan {
   double *d_seeds = nullptr;
   double *d_xbuf = nullptr;
   wm::DevRing *d_rings = nullptr;
+  double *d_twiddles = nullptr, *d_filters = nullptr;
+  int32_t twlen = 0, ring_smem = 0, max_bluestein = 0;
   double *d_alm = nullptr, *d_map = nullptr, *d_q = nullptr, *d_scratch = nullptr;
   int64_t slot_stride = 0;
   cudaStream_t stream = nullptr;
@@ -141,7 +143,15 @@ bool read_file(const std::string &path, std::vector<char> &buf, std::string &err
   return true;
 }
 
-std::vector<wm::DevRing> ring_table(int nside) {
+struct RingTable {
+  std::vector<wm::DevRing> rings;
+  int64_t filter_cplx = 0;   // complex entries of all Bluestein filter spectra
+  int32_t twlen = 2;         // largest power-of-two transform length
+  int32_t smem_cplx = 0;     // largest shared-memory need of a ring CTA
+  int32_t max_bluestein = 0;
+};
+
+RingTable ring_table(int nside) {
   const int nrings = 4 * nside - 1, mid = 2 * nside - 1;
   std::vector<int64_t> offs(nrings + 1);
   int64_t ipix = 0, npr = 0;
@@ -163,7 +173,8 @@ std::vector<wm::DevRing> ring_table(int nside) {
     ipix += npr;
   }
   offs[nrings] = ipix;
-  std::vector<wm::DevRing> out(2 * nside);
+  RingTable T;
+  T.rings.resize(2 * nside);
   for (int r = 0; r < 2 * nside; ++r) {
     wm::DevRing R{};
     R.n = (int32_t)(offs[mid + r + 1] - offs[mid + r]);
@@ -171,10 +182,25 @@ std::vector<wm::DevRing> ring_table(int nside) {
     R.phi_den = den[mid + r];
     R.off_north = offs[mid - r];
     R.off_south = offs[mid + r];
-    out[r] = R;
+    const int N = R.n / 2;
+    int len = N;
+    if (N & (N - 1)) {
+      int M = 1;
+      while (M < 2 * N - 1) M <<= 1;
+      R.bluestein_m = M;
+      R.filter = T.filter_cplx;
+      T.filter_cplx += M;
+      T.max_bluestein = std::max(T.max_bluestein, M);
+      len = M;
+    }
+    T.twlen = std::max(T.twlen, len);
+    T.smem_cplx = std::max(T.smem_cplx, N + 1 + len);
+    T.rings[r] = R;
   }
-  return out;
+  return T;
 }
+
+wm::RingParams ring_params(wavemoth_plan P);
 
 wm::FastParams fast_params(wavemoth_plan P) {
   const auto &G = P->prog;
@@ -295,7 +321,16 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   rc = rc ? rc : A.alloc(&P->d_seeds, (size_t)std::max<int64_t>(G.nseeds, 1), "recurrence seeds");
   P->program_bytes = A.bytes;
   rc = rc ? rc : A.alloc(&P->d_xbuf, (size_t)std::max<int64_t>(G.xrows, 1) * P->nvecs, "X buffer");
-  rc = rc ? rc : upload(A, &P->d_rings, ring_table(P->nside), "ring table");
+  {
+    RingTable RT = ring_table(P->nside);
+    P->twlen = RT.twlen;
+    P->ring_smem = RT.smem_cplx;
+    P->max_bluestein = RT.max_bluestein;
+    rc = rc ? rc : upload(A, &P->d_rings, RT.rings, "ring table");
+    rc = rc ? rc : A.alloc(&P->d_twiddles, (size_t)RT.twlen, "twiddle table");
+    rc = rc ? rc : A.alloc(&P->d_filters, (size_t)std::max<int64_t>(2 * RT.filter_cplx, 2),
+                           "Bluestein filters");
+  }
   rc = rc ? rc : A.alloc(&P->d_counter, 1, "counter");
   rc = rc ? rc : A.alloc(&P->d_q, (size_t)2 * (mmax + 1) * P->ni * P->nvecs, "q buffer");
   rc = rc ? rc : A.alloc(&P->d_scratch, (size_t)P->grid * P->slot_stride, "butterfly scratch");
@@ -305,6 +340,12 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   }
   rc = rc ? rc : cuda_check(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking),
                             "cudaStreamCreate");
+  if (!rc) {
+    wm::RingParams rp = ring_params(P);
+    rc = cuda_check(wm::launch_ring_setup(rp, P->d_twiddles, P->max_bluestein ? P->d_filters : nullptr,
+                                          P->stream), "ring setup launch");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "ring setup");
+  }
   if (!rc && G.nseeds > 0) {
     wm::FastParams fp = fast_params(P);
     fp.seeds_out = P->d_seeds;
@@ -378,6 +419,11 @@ wm::RingParams ring_params(wavemoth_plan P) {
   r.nvecs = P->nvecs;
   r.scale = 4.0 * 3.14159265358979323846 / (double)P->npix;
   r.phase_shifts = P->phase_shifts;
+  r.twiddles = reinterpret_cast<const double2 *>(P->d_twiddles);
+  r.twlen = P->twlen;
+  r.filters = P->d_filters;
+  r.smem_cplx = P->ring_smem;
+  r.max_bluestein_m = P->max_bluestein;
   return r;
 }
 

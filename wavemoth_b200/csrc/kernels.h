@@ -74,10 +74,18 @@ struct RingParams {
   double *q_out;          // analysis output
   double scale;           // analysis: multiplies q~ (4 pi / npix for map2alm)
   int32_t phase_shifts;   // 0 disables e^{i m phi0} (test hook)
+  const double2 *twiddles;  // e^{2 pi i k / twlen}, k < twlen / 2
+  int32_t twlen;
+  const double *filters;  // Bluestein filter spectra (complex, bit-reversed)
+  double *filters_out;    // written at plan creation
+  int32_t smem_cplx;      // complex entries of shared memory per CTA
+  int32_t max_bluestein_m;
 };
 
-size_t ring_smem_bytes(int nside);
+size_t ring_smem_bytes(int max_cplx);
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st);
+cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
+                              cudaStream_t st);
 
 }  // namespace wm

@@ -33,8 +33,8 @@ namespace {
 
 constexpr int kThr = 256;        // 8 warps
 constexpr int kKC = 32;          // alm2map residual: rows per K chunk
-constexpr int kTileCols = 64;    // alm2map residual: columns per tile (8 M-tiles)
-constexpr int kPushCols = 64;    // map2alm residual: columns per K chunk
+constexpr int kTileCols = 256;   // alm2map residual: columns per tile (32 M-tiles)
+constexpr int kPushCols = 256;   // map2alm residual: columns per K chunk
 
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -63,15 +63,20 @@ __device__ __forceinline__ double w_elem(const int32_t *map, const double *ip_t,
 }
 
 // ------------------------------------------------------------------------
-// alm2map residual: one unit = <= 64 columns of one group, all rows.
+// alm2map residual: one unit = <= 256 columns of one group, all rows.  Every
+// thread generates one column of the recurrence tile; warp w owns M-tiles
+// w, w+8, w+16, w+24 (columns 8 mt ..) for all NT vector tiles.  The next
+// chunk of alm rows is prefetched into registers during the products.
 // ------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(kThr) k_a2m_residual(FastParams p) {
+__global__ void __launch_bounds__(kThr, 1) k_a2m_residual(FastParams p) {
   constexpr int VT = 8 * NT;
   constexpr int VP = VT + 8;              // padded row stride (conflict-free fragments)
   constexpr int CP = kTileCols + 8;
-  __shared__ double a_tile[kKC][VP];
-  __shared__ double p_tile[kKC][CP];
+  constexpr int PF = (kKC * VT + kThr - 1) / kThr;   // prefetched alm values per thread
+  extern __shared__ double a2m_smem[];
+  double(*a_tile)[VP] = reinterpret_cast<double(*)[VP]>(a2m_smem);
+  double(*p_tile)[CP] = reinterpret_cast<double(*)[CP]>(a2m_smem + kKC * VP);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g4 = lane >> 2, t4 = lane & 3;
   for (int unit = blockIdx.x; unit < p.ntiles_a; unit += gridDim.x) {
@@ -79,78 +84,99 @@ __global__ void __launch_bounds__(kThr) k_a2m_residual(FastParams p) {
     const DevGroup G = p.groups[T.group];
     const DevMatrix M = p.mats[G.matrix];
     const int64_t arow0 = alm_row0(M, p.lmax);
-    // this thread's column (generation)
-    const bool gen = threadIdx.x < T.ncols;
+    const int c = threadIdx.x;
+    const bool gen = c < T.ncols;
     DevGCol C{};
     double x2 = 0.0, pp = 0.0, pc = 0.0;
     if (gen) {
-      C = p.gcols[G.cols + T.col0 + threadIdx.x];
+      C = p.gcols[G.cols + T.col0 + c];
       if (C.kind == 1 && C.start < G.nrows) {
         x2 = p.f64[C.data];
         pp = p.f64[C.data + C.nx];
         pc = p.f64[C.data + 2 * C.nx];
       }
     }
+    const int nmt = (T.ncols + 7) / 8;
     for (int v0 = 0; v0 < p.nvecs; v0 += VT) {
       const int vn = min(VT, p.nvecs - v0);
-      double acc[NT][2];
+      double acc[4][NT][2];
 #pragma unroll
-      for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
-      // generation state restarts for every vector block
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) acc[i][nt][0] = acc[i][nt][1] = 0.0;
       double gpp = pp, gpc = pc;
+      double pf[PF];
+      auto prefetch = [&](int r0) {
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const int idx = threadIdx.x + j * kThr;
+          const int i = idx / VT, v = idx % VT, r = r0 + i;
+          pf[j] = (idx < kKC * VT && r < G.nrows && v < vn)
+                      ? p.alm_in[(arow0 + 2 * (int64_t)(G.rs + r)) * p.nvecs + v0 + v]
+                      : 0.0;
+        }
+      };
+      prefetch(T.kstart);
       for (int r0 = T.kstart; r0 < G.nrows; r0 += kKC) {
-        for (int idx = threadIdx.x; idx < kKC * VT; idx += kThr) {
-          const int i = idx / VT, v = idx % VT;
+        __syncthreads();   // previous products done with both tiles
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+          const int idx = threadIdx.x + j * kThr;
+          if (idx < kKC * VT) a_tile[idx / VT][idx % VT] = pf[j];
+        }
+        for (int i = 0; i < kKC; ++i) {
           const int r = r0 + i;
           double val = 0.0;
-          if (r < G.nrows && v < vn) val = p.alm_in[(arow0 + 2 * (int64_t)(G.rs + r)) * p.nvecs + v0 + v];
-          a_tile[i][v] = val;
-        }
-        if (threadIdx.x < kTileCols) {
-          const int c = threadIdx.x;
-          for (int i = 0; i < kKC; ++i) {
-            const int r = r0 + i;
-            double val = 0.0;
-            if (gen && r >= C.start && r < G.nrows) {
-              if (C.kind == 0) {
-                val = p.f64[C.data + (r - C.start)];
-              } else if (r == C.start) {
-                val = gpp;
-              } else if (r == C.start + 1) {
-                val = gpc;
-              } else {
-                const double nv = rec_step(p.f64, C, x2, r, gpc, gpp);
-                gpp = gpc;
-                gpc = nv;
-                val = nv;
-              }
+          if (gen && r >= C.start && r < G.nrows) {
+            if (C.kind == 0) {
+              val = p.f64[C.data + (r - C.start)];
+            } else if (r == C.start) {
+              val = gpp;
+            } else if (r == C.start + 1) {
+              val = gpc;
+            } else {
+              const double nv = rec_step(p.f64, C, x2, r, gpc, gpp);
+              gpp = gpc;
+              gpc = nv;
+              val = nv;
             }
-            p_tile[i][c] = val;
           }
+          p_tile[i][c] = val;
         }
         __syncthreads();
+        if (r0 + kKC < G.nrows) prefetch(r0 + kKC);
 #pragma unroll 2
         for (int ks = 0; ks < kKC / 4; ++ks) {
-          const double a = p_tile[4 * ks + t4][8 * warp + g4];
+          double b[NT];
 #pragma unroll
-          for (int nt = 0; nt < NT; ++nt) dmma(acc[nt], a, a_tile[4 * ks + t4][8 * nt + g4]);
+          for (int nt = 0; nt < NT; ++nt) b[nt] = a_tile[4 * ks + t4][8 * nt + g4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int mt = warp + 8 * i;
+            if (mt >= nmt) break;
+            const double a = p_tile[4 * ks + t4][8 * mt + g4];
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) dmma(acc[i][nt], a, b[nt]);
+          }
         }
-        __syncthreads();
       }
-      // epilogue: column 8 warp + g4, vectors 8 nt + 2 t4 + {0, 1}
-      const int c = 8 * warp + g4;
-      if (c < T.ncols) {
-        const DevGCol Co = p.gcols[G.cols + T.col0 + c];
-        double *dst = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs
-                             : p.xbuf + M.xrow * p.nvecs;
-        dst += (int64_t)Co.row * p.nvecs + v0;
+      // epilogue: column 8 mt + g4, vectors 8 nt + 2 t4 + {0, 1}
+      double *base = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs
+                            : p.xbuf + M.xrow * p.nvecs;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int cc = 8 * (warp + 8 * i) + g4;
+        if (cc >= T.ncols) continue;
+        const DevGCol Co = p.gcols[G.cols + T.col0 + cc];
+        double *dst = base + (int64_t)Co.row * p.nvecs + v0;
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
           const int v = 8 * nt + 2 * t4;
-          if (v < vn) dst[v] = acc[nt][0];
-          if (v + 1 < vn) dst[v + 1] = acc[nt][1];
+          if (v < vn) dst[v] = acc[i][nt][0];
+          if (v + 1 < vn) dst[v + 1] = acc[i][nt][1];
         }
       }
+      __syncthreads();
     }
   }
 }
@@ -287,7 +313,7 @@ __global__ void __launch_bounds__(kThr) k_m2a_level(FastParams p) {
 // map2alm residual: one unit = kPushRows rows of one group, all its columns.
 // ------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(kThr) k_m2a_residual(FastParams p) {
+__global__ void __launch_bounds__(kThr, 1) k_m2a_residual(FastParams p) {
   constexpr int VT = 8 * NT;
   constexpr int VP = VT + 8;
   constexpr int PP = kPushCols + 4;       // rows of 8 fragments hit all banks
@@ -314,7 +340,7 @@ __global__ void __launch_bounds__(kThr) k_m2a_residual(FastParams p) {
         const int nc = min(kPushCols, G.ncols - c0);
         __syncthreads();
         // recurrence tile: thread c generates column c0 + c for the unit's rows
-        if (threadIdx.x < kPushCols) {
+        {
           const int c = threadIdx.x;
           if (c < nc) {
             const DevGCol C = p.gcols[G.cols + c0 + c];
@@ -349,14 +375,13 @@ __global__ void __launch_bounds__(kThr) k_m2a_residual(FastParams p) {
             for (int i = 0; i < kPushRows; ++i) p_tile[i][c] = 0.0;
           }
         }
-        for (int idx = threadIdx.x; idx < kPushCols * VT; idx += kThr) {
-          const int c = idx / VT, v = idx % VT;
-          double val = 0.0;
-          if (c < nc && v < vn) {
-            const int row = p.gcols[G.cols + c0 + c].row;
-            val = Xb[(int64_t)row * p.nvecs + v0 + v];
-          }
-          x_tile[c][v] = val;
+        {
+          // each thread stages one column (row of X) of the chunk
+          const int c = threadIdx.x;
+          const double *src = (c < nc) ? Xb + (int64_t)p.gcols[G.cols + c0 + c].row * p.nvecs + v0
+                                       : nullptr;
+#pragma unroll 8
+          for (int v = 0; v < VT; ++v) x_tile[c][v] = (src && v < vn) ? src[v] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -428,9 +453,14 @@ __global__ void k_seeds(FastParams p) {
 template <int NT>
 cudaError_t launch_nt(int which, const FastParams &prm, int grid, size_t smem, cudaStream_t st) {
   switch (which) {
-    case 0:
-      k_a2m_residual<NT><<<grid, kThr, 0, st>>>(prm);
+    case 0: {
+      const size_t sm = (size_t)(kKC * (8 * NT + 8) + kKC * (kTileCols + 8)) * sizeof(double);
+      cudaError_t e = cudaFuncSetAttribute(k_a2m_residual<NT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      k_a2m_residual<NT><<<grid, kThr, sm, st>>>(prm);
       break;
+    }
     case 1: {
       cudaError_t e = cudaFuncSetAttribute(k_a2m_level<NT>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

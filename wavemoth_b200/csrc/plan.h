@@ -124,9 +124,11 @@ struct DevRing {
   int32_t n;              // pixels in the ring
   int32_t phi_num;        // phi0 = pi * phi_num / phi_den
   int32_t phi_den;
-  int32_t pad;
+  int32_t bluestein_m;    // 0: n/2 is a power of two; else the Bluestein convolution length
   int64_t off_north;      // first pixel of ring mid - r
   int64_t off_south;      // first pixel of ring mid + r (== off_north at the equator)
+  int64_t filter;         // Bluestein: complex offset of the filter spectrum (bit-reversed)
+  int64_t pad;
 };
 
 // Device-resident error word (never trap: kernels record and return).

@@ -542,8 +542,10 @@ bool build_fast_path(HostProgram &P, std::string &err) {
       P.nseeds += 2LL * G.ncols * G.nchunks;
       const int32_t gi = (int32_t)P.groups.size();
       P.groups.push_back(G);
-      for (int32_t c0 = 0; c0 < G.ncols; c0 += 64) {
-        DevTileA T{gi, c0, std::min(64, G.ncols - c0), G.nrows};
+      const int32_t ntiles = (G.ncols + 255) / 256;
+      const int32_t width = ntiles ? ((G.ncols + ntiles - 1) / ntiles + 7) & ~7 : 8;
+      for (int32_t c0 = 0; c0 < G.ncols; c0 += width) {
+        DevTileA T{gi, c0, std::min(width, G.ncols - c0), G.nrows};
         for (int32_t c = c0; c < c0 + T.ncols; ++c)
           T.kstart = std::min(T.kstart, P.gcols[G.cols + c].start);
         T.kstart &= ~3;

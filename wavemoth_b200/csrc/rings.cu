@@ -12,15 +12,26 @@
 // The c2r of even length n = 2N runs as one complex inverse FFT of length N:
 //   Z[k] = (W[k] + conj W[N-k]) + i w^k (W[k] - conj W[N-k]),  w = e^{2 pi i / n}
 //   ring[2s] = Re z[s], ring[2s+1] = Im z[s],  z = IDFT_N(Z)
-// and the analysis r2c uses the mirror identity.  The length-N transform is
-// a mixed-radix Stockham autosort FFT in shared memory (radix 4, 2, 3, 5, 7
-// butterflies in registers; any other prime factor p through a length-p DFT
-// per output from the table of roots).  All twiddles come from one table of
-// n-th roots of unity computed with sincospi on exact rationals.
+// and the analysis r2c uses the mirror identity.
+//
+// Length-N transforms, in place in one shared-memory buffer:
+//   * N a power of two (every belt ring): radix-2 Cooley-Tukey.  The inverse
+//     reads its input in bit-reversed order (Z is stored there as it is
+//     formed) and writes natural order; the forward (decimation in
+//     frequency) reads natural order and leaves the spectrum bit-reversed.
+//   * any other N (polar rings, n = 4i): Bluestein's chirp-z identity
+//     jk = (j^2 + k^2 - (k - j)^2) / 2 turns the DFT into a cyclic convolution
+//     of length M = 2^p >= 2N - 1: forward decimation-in-frequency FFT of the
+//     chirped input (bit-reversed spectrum), product with the chirp filter's
+//     spectrum (precomputed per ring at plan creation, stored bit-reversed),
+//     inverse decimation-in-time FFT back to natural order.
+// Twiddles come from one table of e^{2 pi i k / TW}, TW the largest power of
+// two used, computed with sincospi on exact rationals; chirps and the w^k of
+// the real-input identity likewise.
 //
 // One CTA per (map, ring pair), maps fastest in the grid so that the CTAs that
 // share the 32-byte sectors of q (16 bytes per map) and of the interleaved
-// (npix, nmaps) map run at the same time; ring lengths are 4, 8, ..., 4 nside.
+// (npix, nmaps) map run at the same time.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -46,103 +57,94 @@ __device__ __forceinline__ cplx cconj(cplx a) { return {a.x, -a.y}; }
 __device__ __forceinline__ cplx cscale(cplx a, double s) { return {a.x * s, a.y * s}; }
 __device__ __forceinline__ cplx mul_i(cplx a) { return {-a.y, a.x}; }
 
-// e^{2 pi i e / n} from the half table roots[u] = e^{2 pi i u / n}, u < n/2
-__device__ __forceinline__ cplx root(const cplx *roots, int n, long long e) {
-  long long u = e % n;
-  if (u < 0) u += n;
-  const int N = n >> 1;
-  if (u < N) return roots[u];
-  cplx r = roots[u - N];
-  return {-r.x, -r.y};
+__device__ __forceinline__ unsigned bitrev(unsigned k, int bits) {
+  return bits ? (__brev(k) >> (32 - bits)) : 0u;
 }
 
-__device__ __forceinline__ int pick_radix(int rem) {
-  if (rem % 4 == 0) return 4;
-  if (rem % 2 == 0) return 2;
-  if (rem % 3 == 0) return 3;
-  if (rem % 5 == 0) return 5;
-  if (rem % 7 == 0) return 7;
-  int p = 11;
-  while (rem % p) p += 2;
-  return p;
+// e^{sign 2 pi i j / len}, j < len/2, from tw[k] = e^{2 pi i k / TW}
+__device__ __forceinline__ cplx twiddle(const double2 *tw, int twlen, int len, int j, int sign) {
+  const double2 t = tw[(int64_t)j * (twlen / len)];
+  return {t.x, sign * t.y};
 }
 
-// Block-wide complex FFT of length N (unnormalised), sign +1: inverse
-// (e^{+2 pi i jk/N}), -1: forward.  a holds the input; b is scratch of N
-// entries.  Returns the buffer holding the result.  n = 2N is the length of
-// the root table's circle.
-__device__ cplx *block_fft(cplx *a, cplx *b, const cplx *roots, int N, int sign) {
-  const int n = 2 * N;
-  int rem = N, Ns = 1;
-  cplx *in = a, *out = b;
-  while (rem > 1) {
-    const int R = pick_radix(rem);
-    const int NR = N / R;
-    const int tw = n / (Ns * R);
-    const int rot = n / R;  // exponent unit of the radix-R DFT
-    if (R <= 7) {
-      for (int j = threadIdx.x; j < NR; j += blockDim.x) {
-        const int k = j % Ns;
-        cplx v[7];
-        for (int r = 0; r < R; ++r) {
-          cplx x = in[j + r * NR];
-          v[r] = r ? cmul(x, root(roots, n, (long long)sign * r * k * tw)) : x;
-        }
-        cplx V[7];
-        if (R == 2) {
-          V[0] = cadd(v[0], v[1]);
-          V[1] = csub(v[0], v[1]);
-        } else if (R == 4) {
-          cplx s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-          cplx s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
-          cplx id = mul_i(d13);
-          if (sign < 0) id = {-id.x, -id.y};
-          V[0] = cadd(s02, s13);
-          V[2] = csub(s02, s13);
-          V[1] = cadd(d02, id);
-          V[3] = csub(d02, id);
-        } else if (R == 3) {
-          const double c = -0.5, s = 0.86602540378443864676 * sign;
-          cplx s12 = cadd(v[1], v[2]), d12 = csub(v[1], v[2]);
-          cplx base = {v[0].x + c * s12.x, v[0].y + c * s12.y};
-          cplx rot90 = {-s * d12.y, s * d12.x};
-          V[0] = cadd(v[0], s12);
-          V[1] = cadd(base, rot90);
-          V[2] = csub(base, rot90);
-        } else {
-          for (int u = 0; u < R; ++u) {
-            cplx acc = v[0];
-            for (int t = 1; t < R; ++t)
-              acc = cadd(acc, cmul(v[t], root(roots, n, (long long)sign * ((t * u) % R) * rot)));
-            V[u] = acc;
-          }
-        }
-        const int idxD = (j / Ns) * Ns * R + k;
-        for (int r = 0; r < R; ++r) out[idxD + r * Ns] = V[r];
-      }
-    } else {
-      // generic prime radix: twiddle in place, then one output per thread
-      for (int e = threadIdx.x; e < N; e += blockDim.x) {
-        const int j = e % NR, r = e / NR, k = j % Ns;
-        if (r) in[e] = cmul(in[e], root(roots, n, (long long)sign * r * k * tw));
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < N; e += blockDim.x) {
-        const int j = e % NR, u = e / NR, k = j % Ns;
-        cplx acc = {0.0, 0.0};
-        for (int t = 0; t < R; ++t)
-          acc = cadd(acc, cmul(in[j + t * NR], root(roots, n, (long long)sign * ((t * u) % R) * rot)));
-        out[(j / Ns) * Ns * R + k + u * Ns] = acc;
-      }
+__device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
+
+// In-place forward (sign -1) or inverse (+1) DIF: natural in, bit-reversed
+// out.  Consecutive radix-2 stages (len, len/2) are fused into one pass over
+// the data (radix 2^2), which leaves the output order unchanged.
+__device__ void fft_dif(cplx *x, int M, const double2 *tw, int twlen, int sign) {
+  int len = M;
+  for (; len >= 4; len >>= 2) {
+    const int q = len >> 2;
+    for (int b = threadIdx.x; b < M / 4; b += blockDim.x) {
+      const int j = b % q, base = (b / q) * len + j;
+      const cplx a0 = x[base], a1 = x[base + q], a2 = x[base + 2 * q], a3 = x[base + 3 * q];
+      const cplx w1 = twiddle(tw, twlen, len, j, sign), w1b = twiddle(tw, twlen, len, j + q, sign);
+      const cplx w2 = twiddle(tw, twlen, len >> 1, j, sign);
+      const cplx b0 = cadd(a0, a2), b2 = cmul(csub(a0, a2), w1);
+      const cplx b1 = cadd(a1, a3), b3 = cmul(csub(a1, a3), w1b);
+      x[base] = cadd(b0, b1);
+      x[base + q] = cmul(csub(b0, b1), w2);
+      x[base + 2 * q] = cadd(b2, b3);
+      x[base + 3 * q] = cmul(csub(b2, b3), w2);
     }
     __syncthreads();
-    cplx *tmp = in;
-    in = out;
-    out = tmp;
-    Ns *= R;
-    rem /= R;
   }
-  return in;
+  if (len == 2) {
+    for (int b = threadIdx.x; b < M / 2; b += blockDim.x) {
+      const cplx u = x[2 * b], v = x[2 * b + 1];
+      x[2 * b] = cadd(u, v);
+      x[2 * b + 1] = csub(u, v);
+    }
+    __syncthreads();
+  }
+}
+
+// In-place DIT: bit-reversed in, natural out; stages (L, 2L) fused.
+__device__ void fft_dit(cplx *x, int M, const double2 *tw, int twlen, int sign) {
+  int L = 2;
+  if (ilog2(M) & 1) {
+    for (int b = threadIdx.x; b < M / 2; b += blockDim.x) {
+      const cplx u = x[2 * b], v = x[2 * b + 1];
+      x[2 * b] = cadd(u, v);
+      x[2 * b + 1] = csub(u, v);
+    }
+    __syncthreads();
+    L = 4;
+  }
+  for (; L <= M / 2; L <<= 2) {
+    const int q = L >> 1, len = 2 * L;
+    for (int b = threadIdx.x; b < M / 4; b += blockDim.x) {
+      const int j = b % q, base = (b / q) * len + j;
+      const cplx a0 = x[base], a1 = x[base + q], a2 = x[base + 2 * q], a3 = x[base + 3 * q];
+      const cplx w1 = twiddle(tw, twlen, L, j, sign);
+      const cplx w2 = twiddle(tw, twlen, len, j, sign), w2b = twiddle(tw, twlen, len, j + q, sign);
+      const cplx t1 = cmul(a1, w1), t3 = cmul(a3, w1);
+      const cplx b0 = cadd(a0, t1), b1 = csub(a0, t1), b2 = cadd(a2, t3), b3 = csub(a2, t3);
+      const cplx u2 = cmul(b2, w2), u3 = cmul(b3, w2b);
+      x[base] = cadd(b0, u2);
+      x[base + 2 * q] = csub(b0, u2);
+      x[base + q] = cadd(b1, u3);
+      x[base + 3 * q] = csub(b1, u3);
+    }
+    __syncthreads();
+  }
+}
+
+
+// e^{i pi k^2 / N}
+__device__ __forceinline__ cplx chirp(int k, int N) {
+  const long long k2 = ((long long)k * k) % (2LL * N);
+  double s, c;
+  sincospi((double)k2 / (double)N, &s, &c);
+  return {c, s};
+}
+
+// e^{2 pi i k / n}
+__device__ __forceinline__ cplx unit_root(int k, int n) {
+  double s, c;
+  sincospi((double)(2 * k) / (double)n, &s, &c);
+  return {c, s};
 }
 
 __device__ __forceinline__ cplx phase(int m, const DevRing &R, int enabled) {
@@ -154,13 +156,56 @@ __device__ __forceinline__ cplx phase(int m, const DevRing &R, int enabled) {
   return {c, s};
 }
 
-__device__ void build_roots(cplx *roots, int n) {
-  const int N = n / 2;
-  for (int u = threadIdx.x; u < N; u += blockDim.x) {
-    double s, c;
-    sincospi((double)(2 * u) / (double)n, &s, &c);
-    roots[u] = {c, s};
+// Unnormalised length-N DFT with sign (+1 inverse, -1 forward) of the values
+// in `buf`.  Power-of-two N: `buf` holds the input in bit-reversed order
+// (inverse) or natural order (forward); the result is in natural order
+// (inverse) or bit-reversed order (forward).  Other N (Bluestein): `buf` has
+// room for M entries, holds the input in natural order in [0, N) and the
+// result in natural order in [0, N) for both signs.
+__device__ void ring_dft(cplx *buf, const DevRing &R, const RingParams &p, int sign) {
+  const int N = R.n / 2;
+  if (R.bluestein_m == 0) {
+    if (sign > 0) fft_dit(buf, N, p.twiddles, p.twlen, +1);
+    else fft_dif(buf, N, p.twiddles, p.twlen, -1);
+    return;
   }
+  const int M = R.bluestein_m;
+  // chirp with w^{-sign}: x_k w_k^{sign}, zero padded
+  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+    cplx v = {0.0, 0.0};
+    if (k < N) {
+      cplx w = chirp(k, N);
+      if (sign < 0) w = cconj(w);
+      v = cmul(buf[k], w);
+    }
+    buf[k] = v;
+  }
+  __syncthreads();
+  fft_dif(buf, M, p.twiddles, p.twlen, -1);
+  // product with the filter spectrum (stored bit-reversed for sign +1; the
+  // sign -1 filter is its complex conjugate reflected: F'(p) = conj F(-p))
+  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + R.filter;
+  const int bits = ilog2(M);
+  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+    cplx f;
+    if (sign > 0) {
+      f = F[k];
+    } else {
+      const unsigned natural = bitrev((unsigned)k, bits);
+      const unsigned refl = (M - natural) & (M - 1);
+      f = cconj(F[bitrev(refl, bits)]);
+    }
+    buf[k] = cmul(buf[k], f);
+  }
+  __syncthreads();
+  fft_dit(buf, M, p.twiddles, p.twlen, +1);
+  const double inv = 1.0 / (double)M;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    cplx w = chirp(k, N);
+    if (sign < 0) w = cconj(w);
+    buf[k] = cscale(cmul(buf[k], w), inv);
+  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
@@ -169,14 +214,13 @@ __global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
   const int kmap = blockIdx.x, r = blockIdx.y;
   const DevRing R = p.rings[r];
   const int n = R.n, N = n / 2;
-  cplx *bufA = sm;
-  cplx *bufB = sm + (N + 1);
-  cplx *roots = bufB + (N + 1);
-  build_roots(roots, n);
-  const int64_t qstride_m = 2LL * p.ni * p.nvecs;       // q[(2m + odd) * ni * nvecs]
+  const int bits = ilog2(N);
+  const bool pow2 = R.bluestein_m == 0;
+  cplx *W = sm;            // N + 1
+  cplx *buf = sm + N + 1;  // N or M
+  const int64_t qstride_m = 2LL * p.ni * p.nvecs;  // q[(2m + odd) * ni * nvecs]
   const int64_t qoff = (int64_t)r * p.nvecs + 2 * kmap;
   const int64_t half = (int64_t)p.ni * p.nvecs;
-  __syncthreads();
   for (int side = 0; side < 2; ++side) {
     if (side == 1 && r == 0) break;  // the equator is written once
     const double sgn = side ? -1.0 : 1.0;
@@ -199,23 +243,24 @@ __global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
           acc = cadd(acc, cconj(cmul(t, phase(m2, R, p.phase_shifts))));
         }
       }
-      bufA[j] = acc;
+      W[j] = acc;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
-      cplx Wk = bufA[k], Wc = cconj(bufA[N - k]);
+      cplx Wk = W[k], Wc = cconj(W[N - k]);
       if (k == 0) {
         Wk.y = 0.0;
         Wc.y = 0.0;
       }
-      cplx s = cadd(Wk, Wc), d = csub(Wk, Wc);
-      bufB[k] = cadd(s, mul_i(cmul(root(roots, n, k), d)));
+      const cplx s = cadd(Wk, Wc), d = csub(Wk, Wc);
+      const cplx Z = cadd(s, mul_i(cmul(unit_root(k, n), d)));
+      buf[pow2 ? bitrev((unsigned)k, bits) : k] = Z;
     }
     __syncthreads();
-    cplx *res = block_fft(bufB, bufA, roots, N, +1);
+    ring_dft(buf, R, p, +1);
     const int64_t off = side ? R.off_south : R.off_north;
     for (int s = threadIdx.x; s < N; s += blockDim.x) {
-      cplx z = res[s];
+      const cplx z = buf[s];
       p.map[(off + 2 * s) * p.nmaps + kmap] = z.x;
       p.map[(off + 2 * s + 1) * p.nmaps + kmap] = z.y;
     }
@@ -229,28 +274,29 @@ __global__ void __launch_bounds__(kRingThreads) k_ring_analysis(RingParams p) {
   const int kmap = blockIdx.x, r = blockIdx.y;
   const DevRing R = p.rings[r];
   const int n = R.n, N = n / 2;
-  cplx *bufA = sm;
-  cplx *bufB = sm + (N + 1);
-  cplx *roots = bufB + (N + 1);
-  build_roots(roots, n);
+  const int bits = ilog2(N);
+  const bool pow2 = R.bluestein_m == 0;
+  cplx *F = sm;            // N + 1
+  cplx *buf = sm + N + 1;  // N or M
   const int64_t qstride_m = 2LL * p.ni * p.nvecs;
   const int64_t qoff = (int64_t)r * p.nvecs + 2 * kmap;
   const int64_t half = (int64_t)p.ni * p.nvecs;
-  __syncthreads();
   for (int side = 0; side < 2; ++side) {
     if (side == 1 && r == 0) break;
     const int64_t off = side ? R.off_south : R.off_north;
     for (int s = threadIdx.x; s < N; s += blockDim.x)
-      bufA[s] = {p.map_in[(off + 2 * s) * p.nmaps + kmap], p.map_in[(off + 2 * s + 1) * p.nmaps + kmap]};
+      buf[s] = {p.map_in[(off + 2 * s) * p.nmaps + kmap], p.map_in[(off + 2 * s + 1) * p.nmaps + kmap]};
     __syncthreads();
-    cplx *Z = block_fft(bufA, bufB, roots, N, -1);
-    cplx *F = (Z == bufA) ? bufB : bufA;
+    ring_dft(buf, R, p, -1);
+    // Z in natural order (Bluestein) or bit-reversed (power of two)
     for (int k = threadIdx.x; k <= N; k += blockDim.x) {
-      cplx Zk = Z[k % N], Zc = cconj(Z[(N - k) % N]);
-      cplx E = cscale(cadd(Zk, Zc), 0.5);
-      cplx D = csub(Zk, Zc);
-      cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
-      F[k] = cadd(E, cmul(cconj(root(roots, n, k)), O));
+      const int k1 = k % N, k2 = (N - k) % N;
+      const cplx Zk = buf[pow2 ? bitrev((unsigned)k1, bits) : k1];
+      const cplx Zc = cconj(buf[pow2 ? bitrev((unsigned)k2, bits) : k2]);
+      const cplx E = cscale(cadd(Zk, Zc), 0.5);
+      const cplx D = csub(Zk, Zc);
+      const cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
+      F[k] = cadd(E, cmul(cconj(unit_root(k, n)), O));
     }
     __syncthreads();
     for (int m = threadIdx.x; m <= p.mmax; m += blockDim.x) {
@@ -271,15 +317,40 @@ __global__ void __launch_bounds__(kRingThreads) k_ring_analysis(RingParams p) {
   }
 }
 
-}  // namespace
-
-size_t ring_smem_bytes(int nside) {
-  const size_t N = 2 * (size_t)nside;
-  return (3 * N + 2) * sizeof(double) * 2;
+// Plan creation: twiddle table and the Bluestein filter spectra.
+__global__ void k_twiddles(double2 *tw, int twlen) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < twlen / 2; k += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi((double)(2 * k) / (double)twlen, &s, &c);
+    tw[k] = make_double2(c, s);
+  }
 }
 
+__global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p) {
+  extern __shared__ double smem_d[];
+  cplx *buf = reinterpret_cast<cplx *>(smem_d);
+  const DevRing R = p.rings[blockIdx.x];
+  if (R.bluestein_m == 0) return;
+  const int N = R.n / 2, M = R.bluestein_m;
+  // b_k = conj(e^{i pi k^2 / N}) for k in (-N, N), cyclically placed
+  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+    cplx v = {0.0, 0.0};
+    if (k < N) v = cconj(chirp(k, N));
+    else if (k > M - N) v = cconj(chirp(M - k, N));
+    buf[k] = v;
+  }
+  __syncthreads();
+  fft_dif(buf, M, p.twiddles, p.twlen, -1);
+  cplx *F = reinterpret_cast<cplx *>(p.filters_out) + R.filter;
+  for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[k];
+}
+
+}  // namespace
+
+size_t ring_smem_bytes(int max_cplx) { return (size_t)max_cplx * sizeof(double) * 2; }
+
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
-  const size_t smem = ring_smem_bytes(prm.nside);
+  const size_t smem = ring_smem_bytes(prm.smem_cplx);
   cudaError_t e = cudaFuncSetAttribute(k_ring_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
@@ -289,12 +360,27 @@ cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
 }
 
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
-  const size_t smem = ring_smem_bytes(prm.nside);
+  const size_t smem = ring_smem_bytes(prm.smem_cplx);
   cudaError_t e = cudaFuncSetAttribute(k_ring_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid(prm.nmaps, prm.ni);
   k_ring_analysis<<<grid, kRingThreads, smem, st>>>(prm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
+                              cudaStream_t st) {
+  k_twiddles<<<64, 256, 0, st>>>(reinterpret_cast<double2 *>(twiddles), prm.twlen);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !filters) return e;
+  RingParams q = prm;
+  q.twiddles = reinterpret_cast<const double2 *>(twiddles);
+  q.filters_out = filters;
+  const size_t smem = ring_smem_bytes(prm.max_bluestein_m);
+  e = cudaFuncSetAttribute(k_bluestein_filters, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_bluestein_filters<<<prm.ni, kRingThreads, smem, st>>>(q);
   return cudaGetLastError();
 }
 
