@@ -86,8 +86,10 @@ struct _wavemoth_plan {
   double *d_seeds = nullptr;
   double *d_xbuf = nullptr;
   wm::DevRing *d_rings = nullptr;
-  double *d_twiddles = nullptr, *d_filters = nullptr;
-  int32_t twlen = 0, ring_smem = 0, max_bluestein = 0;
+  wm::DevRingTask *d_ring_tasks = nullptr;
+  double *d_twiddles = nullptr, *d_filters = nullptr, *d_ring_aux = nullptr;
+  int32_t twlen = 0, max_bluestein = 0;
+  int32_t ring_ntasks0 = 0, ring_ntasks1 = 0, ring_smem0 = 0, ring_smem1 = 0, nphase_hi = 1;
   double *d_alm = nullptr, *d_map = nullptr, *d_q = nullptr, *d_scratch = nullptr;
   int64_t slot_stride = 0;
   cudaStream_t stream = nullptr;
@@ -145,13 +147,21 @@ bool read_file(const std::string &path, std::vector<char> &buf, std::string &err
 
 struct RingTable {
   std::vector<wm::DevRing> rings;
+  std::vector<wm::DevRingTask> tasks;  // class 0, then class 1
   int64_t filter_cplx = 0;   // complex entries of all Bluestein filter spectra
-  int32_t twlen = 2;         // largest power-of-two transform length
-  int32_t smem_cplx = 0;     // largest shared-memory need of a ring CTA
+  int64_t aux_cplx = 0;      // complex entries of all Bluestein chirp/root tables
+  int32_t twlen = 4;         // largest power-of-two table length needed
   int32_t max_bluestein = 0;
+  int32_t ntasks0 = 0, ntasks1 = 0;
+  int32_t smem0 = 0, smem1 = 0;
+  int32_t nphase_hi = 1;
 };
 
-RingTable ring_table(int nside) {
+// Ring geometry (src/wavemoth.c:1199-1232) and the CTA work list of the ring
+// kernels: per ring pair, groups of G maps with G x (transform length) within
+// the class-0 shared-memory budget; longer transforms run one map per CTA in
+// class 1.  Each class is ordered by decreasing cost.
+RingTable ring_table(int nside, int nmaps, int mmax) {
   const int nrings = 4 * nside - 1, mid = 2 * nside - 1;
   std::vector<int64_t> offs(nrings + 1);
   int64_t ipix = 0, npr = 0;
@@ -175,6 +185,11 @@ RingTable ring_table(int nside) {
   offs[nrings] = ipix;
   RingTable T;
   T.rings.resize(2 * nside);
+  T.nphase_hi = mmax / 64 + 1;
+  int gmax = 1;
+  while (gmax < nmaps && gmax < 8) gmax <<= 1;
+  struct Item { double cost; wm::DevRingTask t; int cls; int64_t cplx; };
+  std::vector<Item> items;
   for (int r = 0; r < 2 * nside; ++r) {
     wm::DevRing R{};
     R.n = (int32_t)(offs[mid + r + 1] - offs[mid + r]);
@@ -190,13 +205,37 @@ RingTable ring_table(int nside) {
       R.bluestein_m = M;
       R.filter = T.filter_cplx;
       T.filter_cplx += M;
+      R.aux = T.aux_cplx;
+      T.aux_cplx += 2 * N + 1;
       T.max_bluestein = std::max(T.max_bluestein, M);
       len = M;
+      T.twlen = std::max(T.twlen, M);
+    } else {
+      T.twlen = std::max(T.twlen, 2 * N);  // roots e^{2 pi i k / n}, n = 2N
     }
-    T.twlen = std::max(T.twlen, len);
-    T.smem_cplx = std::max(T.smem_cplx, N + 1 + len);
     T.rings[r] = R;
+    int G = 1, cls = 1;
+    if (len <= wm::kRingBufferCplx) {
+      cls = 0;
+      G = std::min(gmax, wm::kRingBufferCplx / len);
+    }
+    int lg = 0;
+    while ((1 << lg) < G) ++lg;
+    const double cost = (double)G * len * (R.bluestein_m ? 2.5 : 1.0) + (double)G * (mmax + 1);
+    for (int g0 = 0; g0 < nmaps; g0 += G)
+      items.push_back({cost, wm::DevRingTask{r, g0, lg, 0}, cls, (int64_t)G * len});
   }
+  std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
+    return a.cls != b.cls ? a.cls < b.cls : a.cost > b.cost;
+  });
+  int64_t need[2] = {0, 0};
+  for (const Item &it : items) {
+    T.tasks.push_back(it.t);
+    (it.cls ? T.ntasks1 : T.ntasks0)++;
+    need[it.cls] = std::max(need[it.cls], it.cplx);
+  }
+  T.smem0 = T.ntasks0 ? wm::ring_cta_smem(need[0], T.nphase_hi) : 0;
+  T.smem1 = T.ntasks1 ? wm::ring_cta_smem(need[1], T.nphase_hi) : 0;
   return T;
 }
 
@@ -322,14 +361,21 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   P->program_bytes = A.bytes;
   rc = rc ? rc : A.alloc(&P->d_xbuf, (size_t)std::max<int64_t>(G.xrows, 1) * P->nvecs, "X buffer");
   {
-    RingTable RT = ring_table(P->nside);
+    RingTable RT = ring_table(P->nside, nmaps, mmax);
     P->twlen = RT.twlen;
-    P->ring_smem = RT.smem_cplx;
     P->max_bluestein = RT.max_bluestein;
+    P->ring_ntasks0 = RT.ntasks0;
+    P->ring_ntasks1 = RT.ntasks1;
+    P->ring_smem0 = RT.smem0;
+    P->ring_smem1 = RT.smem1;
+    P->nphase_hi = RT.nphase_hi;
     rc = rc ? rc : upload(A, &P->d_rings, RT.rings, "ring table");
+    rc = rc ? rc : upload(A, &P->d_ring_tasks, RT.tasks, "ring work list");
     rc = rc ? rc : A.alloc(&P->d_twiddles, (size_t)RT.twlen, "twiddle table");
     rc = rc ? rc : A.alloc(&P->d_filters, (size_t)std::max<int64_t>(2 * RT.filter_cplx, 2),
                            "Bluestein filters");
+    rc = rc ? rc : A.alloc(&P->d_ring_aux, (size_t)std::max<int64_t>(2 * RT.aux_cplx, 2),
+                           "Bluestein chirps");
   }
   rc = rc ? rc : A.alloc(&P->d_counter, 1, "counter");
   rc = rc ? rc : A.alloc(&P->d_q, (size_t)2 * (mmax + 1) * P->ni * P->nvecs, "q buffer");
@@ -343,7 +389,7 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   if (!rc) {
     wm::RingParams rp = ring_params(P);
     rc = cuda_check(wm::launch_ring_setup(rp, P->d_twiddles, P->max_bluestein ? P->d_filters : nullptr,
-                                          P->stream), "ring setup launch");
+                                          P->d_ring_aux, P->stream), "ring setup launch");
     if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "ring setup");
   }
   if (!rc && G.nseeds > 0) {
@@ -422,8 +468,14 @@ wm::RingParams ring_params(wavemoth_plan P) {
   r.twiddles = reinterpret_cast<const double2 *>(P->d_twiddles);
   r.twlen = P->twlen;
   r.filters = P->d_filters;
-  r.smem_cplx = P->ring_smem;
+  r.aux = reinterpret_cast<const double2 *>(P->d_ring_aux);
   r.max_bluestein_m = P->max_bluestein;
+  r.tasks = P->d_ring_tasks;
+  r.ntasks0 = P->ring_ntasks0;
+  r.ntasks1 = P->ring_ntasks1;
+  r.smem0 = P->ring_smem0;
+  r.smem1 = P->ring_smem1;
+  r.nphase_hi = P->nphase_hi;
   return r;
 }
 

@@ -78,14 +78,24 @@ struct RingParams {
   int32_t twlen;
   const double *filters;  // Bluestein filter spectra (complex, bit-reversed)
   double *filters_out;    // written at plan creation
-  int32_t smem_cplx;      // complex entries of shared memory per CTA
+  const double2 *aux;     // Bluestein chirps and roots of unity per ring
+  double *aux_out;        // written at plan creation
   int32_t max_bluestein_m;
+  // CTA work list: class 0 (tasks [0, ntasks0)) then class 1, each launched
+  // with its own dynamic shared memory size
+  const DevRingTask *tasks;
+  int32_t ntasks0, ntasks1;
+  int32_t smem0, smem1;   // bytes
+  int32_t nphase_hi;      // entries of the coarse phase table (mmax / 64 + 1)
 };
 
-size_t ring_smem_bytes(int max_cplx);
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
-                              cudaStream_t st);
+                              double *aux, cudaStream_t st);
+// Shared-memory bytes of a ring CTA whose transform buffer holds `cplx`
+// complex values per map lane times the lanes.
+int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi);
+constexpr int32_t kRingBufferCplx = 4096;  // class-0 budget: 64 KB of transform buffer
 
 }  // namespace wm

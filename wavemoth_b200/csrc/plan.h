@@ -128,7 +128,15 @@ struct DevRing {
   int64_t off_north;      // first pixel of ring mid - r
   int64_t off_south;      // first pixel of ring mid + r (== off_north at the equator)
   int64_t filter;         // Bluestein: complex offset of the filter spectrum (bit-reversed)
-  int64_t pad;
+  int64_t aux;            // Bluestein: complex offset of chirp[n/2] then root[n/2 + 1]
+};
+
+// One CTA of a ring kernel: ring pair `ring`, maps [map0, map0 + 2^lg).
+struct DevRingTask {
+  int32_t ring;
+  int32_t map0;
+  int32_t lg;
+  int32_t pad;
 };
 
 // Device-resident error word (never trap: kernels record and return).

@@ -14,10 +14,10 @@
 //   ring[2s] = Re z[s], ring[2s+1] = Im z[s],  z = IDFT_N(Z)
 // and the analysis r2c uses the mirror identity.
 //
-// Length-N transforms, in place in one shared-memory buffer:
-//   * N a power of two (every belt ring): radix-2 Cooley-Tukey.  The inverse
-//     reads its input in bit-reversed order (Z is stored there as it is
-//     formed) and writes natural order; the forward (decimation in
+// Length-N transforms, in place in shared memory:
+//   * N a power of two (every belt ring): radix-2^2 Cooley-Tukey passes.  The
+//     inverse reads its input in bit-reversed order (Z is stored there as it
+//     is formed) and writes natural order; the forward (decimation in
 //     frequency) reads natural order and leaves the spectrum bit-reversed.
 //   * any other N (polar rings, n = 4i): Bluestein's chirp-z identity
 //     jk = (j^2 + k^2 - (k - j)^2) / 2 turns the DFT into a cyclic convolution
@@ -26,12 +26,22 @@
 //     spectrum (precomputed per ring at plan creation, stored bit-reversed),
 //     inverse decimation-in-time FFT back to natural order.
 // Twiddles come from one table of e^{2 pi i k / TW}, TW the largest power of
-// two used, computed with sincospi on exact rationals; chirps and the w^k of
-// the real-input identity likewise.
+// two used; the chirps e^{i pi k^2 / N} and roots e^{2 pi i k / n} of the
+// Bluestein rings from a per-ring table; all are computed once, at plan
+// creation, with sincospi on exact rationals.
 //
-// One CTA per (map, ring pair), maps fastest in the grid so that the CTAs that
-// share the 32-byte sectors of q (16 bytes per map) and of the interleaved
-// (npix, nmaps) map run at the same time.
+// Work decomposition: one CTA per (ring pair, group of G = 2^lg maps), G
+// chosen per ring so that the transform buffer (G x N or G x M complex) fits
+// 64 KB and three CTAs share an SM.  The G maps are the fastest index of the
+// CTA's thread layout: lanes g = 0..G-1 of a warp handle the same bin, pixel
+// or butterfly of G maps, so
+//   * q rows (16 bytes per map, maps adjacent) are read as G x 16-byte runs,
+//   * map pixels (8 bytes per map, maps adjacent) are written as G x 8-byte runs,
+//   * twiddles, chirps and phase factors are shared by the G lanes.
+// In shared memory element i of map lane g is at slot(i) * G + g with the XOR
+// swizzle slot(i) = i ^ ((i >> 3) & 7), a permutation inside each aligned
+// group of 8 that spreads the 16-byte accesses of every radix-4 and radix-2
+// pass over the 32 banks.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,6 +53,7 @@ namespace wm {
 namespace {
 
 constexpr int kRingThreads = 256;
+constexpr int kPhaseLo = 64;  // e^{i m phi0} = hi[m / 64] * lo[m % 64]
 
 struct cplx {
   double x, y;
@@ -56,273 +67,366 @@ __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
 __device__ __forceinline__ cplx cconj(cplx a) { return {a.x, -a.y}; }
 __device__ __forceinline__ cplx cscale(cplx a, double s) { return {a.x * s, a.y * s}; }
 __device__ __forceinline__ cplx mul_i(cplx a) { return {-a.y, a.x}; }
+__device__ __forceinline__ cplx ld2(const double *p) {
+  const double2 v = *reinterpret_cast<const double2 *>(p);
+  return {v.x, v.y};
+}
 
 __device__ __forceinline__ unsigned bitrev(unsigned k, int bits) {
   return bits ? (__brev(k) >> (32 - bits)) : 0u;
 }
 
-// e^{sign 2 pi i j / len}, j < len/2, from tw[k] = e^{2 pi i k / TW}
-__device__ __forceinline__ cplx twiddle(const double2 *tw, int twlen, int len, int j, int sign) {
-  const double2 t = tw[(int64_t)j * (twlen / len)];
+__device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
+
+__device__ __forceinline__ int slot(int i) { return i ^ ((i >> 3) & 7); }
+__device__ __forceinline__ int at(int i, int g, int lg) { return (slot(i) << lg) + g; }
+
+// tw[k] = e^{2 pi i k / twlen}; returns its conjugate for sign -1
+__device__ __forceinline__ cplx twiddle(const double2 *tw, int k, int sign) {
+  const double2 t = tw[k];
   return {t.x, sign * t.y};
 }
 
-__device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
-
-// In-place forward (sign -1) or inverse (+1) DIF: natural in, bit-reversed
-// out.  Consecutive radix-2 stages (len, len/2) are fused into one pass over
-// the data (radix 2^2), which leaves the output order unchanged.
-__device__ void fft_dif(cplx *x, int M, const double2 *tw, int twlen, int sign) {
+// In-place DIF over the 2^lg interleaved sequences of length M (a power of
+// two), natural order in, bit-reversed out.  Consecutive radix-2 stages
+// (len, len/2) are fused into one pass (radix 2^2).
+__device__ void fft_dif(cplx *x, int M, int lg, const double2 *tw, int twlen, int sign) {
+  const int gm = (1 << lg) - 1;
+  const int total = (M >> 2) << lg;
   int len = M;
   for (; len >= 4; len >>= 2) {
-    const int q = len >> 2;
-    for (int b = threadIdx.x; b < M / 4; b += blockDim.x) {
-      const int j = b % q, base = (b / q) * len + j;
-      const cplx a0 = x[base], a1 = x[base + q], a2 = x[base + 2 * q], a3 = x[base + 3 * q];
-      const cplx w1 = twiddle(tw, twlen, len, j, sign), w1b = twiddle(tw, twlen, len, j + q, sign);
-      const cplx w2 = twiddle(tw, twlen, len >> 1, j, sign);
+    const int q = len >> 2, lq = ilog2(q), step = twlen / len;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int g = t & gm, b = t >> lg;
+      const int j = b & (q - 1), base = ((b >> lq) << (lq + 2)) + j;
+      const int i0 = at(base, g, lg), i1 = at(base + q, g, lg);
+      const int i2 = at(base + 2 * q, g, lg), i3 = at(base + 3 * q, g, lg);
+      const cplx a0 = x[i0], a1 = x[i1], a2 = x[i2], a3 = x[i3];
+      const cplx w1 = twiddle(tw, j * step, sign), w1b = twiddle(tw, (j + q) * step, sign);
+      const cplx w2 = twiddle(tw, 2 * j * step, sign);
       const cplx b0 = cadd(a0, a2), b2 = cmul(csub(a0, a2), w1);
       const cplx b1 = cadd(a1, a3), b3 = cmul(csub(a1, a3), w1b);
-      x[base] = cadd(b0, b1);
-      x[base + q] = cmul(csub(b0, b1), w2);
-      x[base + 2 * q] = cadd(b2, b3);
-      x[base + 3 * q] = cmul(csub(b2, b3), w2);
+      x[i0] = cadd(b0, b1);
+      x[i1] = cmul(csub(b0, b1), w2);
+      x[i2] = cadd(b2, b3);
+      x[i3] = cmul(csub(b2, b3), w2);
     }
     __syncthreads();
   }
   if (len == 2) {
-    for (int b = threadIdx.x; b < M / 2; b += blockDim.x) {
-      const cplx u = x[2 * b], v = x[2 * b + 1];
-      x[2 * b] = cadd(u, v);
-      x[2 * b + 1] = csub(u, v);
+    for (int t = threadIdx.x; t < ((M >> 1) << lg); t += blockDim.x) {
+      const int g = t & gm, b = t >> lg;
+      const int i0 = at(2 * b, g, lg), i1 = at(2 * b + 1, g, lg);
+      const cplx u = x[i0], v = x[i1];
+      x[i0] = cadd(u, v);
+      x[i1] = csub(u, v);
     }
     __syncthreads();
   }
 }
 
-// In-place DIT: bit-reversed in, natural out; stages (L, 2L) fused.
-__device__ void fft_dit(cplx *x, int M, const double2 *tw, int twlen, int sign) {
+// In-place DIT over 2^lg interleaved sequences: bit-reversed in, natural out;
+// stages (L, 2L) fused.
+__device__ void fft_dit(cplx *x, int M, int lg, const double2 *tw, int twlen, int sign) {
+  const int gm = (1 << lg) - 1;
+  const int total = (M >> 2) << lg;
   int L = 2;
   if (ilog2(M) & 1) {
-    for (int b = threadIdx.x; b < M / 2; b += blockDim.x) {
-      const cplx u = x[2 * b], v = x[2 * b + 1];
-      x[2 * b] = cadd(u, v);
-      x[2 * b + 1] = csub(u, v);
+    for (int t = threadIdx.x; t < ((M >> 1) << lg); t += blockDim.x) {
+      const int g = t & gm, b = t >> lg;
+      const int i0 = at(2 * b, g, lg), i1 = at(2 * b + 1, g, lg);
+      const cplx u = x[i0], v = x[i1];
+      x[i0] = cadd(u, v);
+      x[i1] = csub(u, v);
     }
     __syncthreads();
     L = 4;
   }
   for (; L <= M / 2; L <<= 2) {
-    const int q = L >> 1, len = 2 * L;
-    for (int b = threadIdx.x; b < M / 4; b += blockDim.x) {
-      const int j = b % q, base = (b / q) * len + j;
-      const cplx a0 = x[base], a1 = x[base + q], a2 = x[base + 2 * q], a3 = x[base + 3 * q];
-      const cplx w1 = twiddle(tw, twlen, L, j, sign);
-      const cplx w2 = twiddle(tw, twlen, len, j, sign), w2b = twiddle(tw, twlen, len, j + q, sign);
+    const int q = L >> 1, lq = ilog2(q), len = 2 * L;
+    const int s1 = twlen / L, s2 = twlen / len;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int g = t & gm, b = t >> lg;
+      const int j = b & (q - 1), base = ((b >> lq) << (lq + 2)) + j;
+      const int i0 = at(base, g, lg), i1 = at(base + q, g, lg);
+      const int i2 = at(base + 2 * q, g, lg), i3 = at(base + 3 * q, g, lg);
+      const cplx a0 = x[i0], a1 = x[i1], a2 = x[i2], a3 = x[i3];
+      const cplx w1 = twiddle(tw, j * s1, sign);
+      const cplx w2 = twiddle(tw, j * s2, sign), w2b = twiddle(tw, (j + q) * s2, sign);
       const cplx t1 = cmul(a1, w1), t3 = cmul(a3, w1);
       const cplx b0 = cadd(a0, t1), b1 = csub(a0, t1), b2 = cadd(a2, t3), b3 = csub(a2, t3);
       const cplx u2 = cmul(b2, w2), u3 = cmul(b3, w2b);
-      x[base] = cadd(b0, u2);
-      x[base + 2 * q] = csub(b0, u2);
-      x[base + q] = cadd(b1, u3);
-      x[base + 3 * q] = csub(b1, u3);
+      x[i0] = cadd(b0, u2);
+      x[i2] = csub(b0, u2);
+      x[i1] = cadd(b1, u3);
+      x[i3] = csub(b1, u3);
     }
     __syncthreads();
   }
 }
 
-
-// e^{i pi k^2 / N}
-__device__ __forceinline__ cplx chirp(int k, int N) {
-  const long long k2 = ((long long)k * k) % (2LL * N);
+// e^{i pi num / den} for an exact rational, reduced modulo 2 first
+__device__ __forceinline__ cplx expi_pi(long long num, long long den) {
+  const long long r = num % (2 * den);
   double s, c;
-  sincospi((double)k2 / (double)N, &s, &c);
+  sincospi((double)r / (double)den, &s, &c);
   return {c, s};
 }
 
-// e^{2 pi i k / n}
-__device__ __forceinline__ cplx unit_root(int k, int n) {
-  double s, c;
-  sincospi((double)(2 * k) / (double)n, &s, &c);
-  return {c, s};
-}
-
-__device__ __forceinline__ cplx phase(int m, const DevRing &R, int enabled) {
-  if (!enabled || R.phi_num == 0) return {1.0, 0.0};
-  const long long den2 = 2LL * R.phi_den;
-  const long long num = ((long long)m * R.phi_num) % den2;
-  double s, c;
-  sincospi((double)num / (double)R.phi_den, &s, &c);
-  return {c, s};
-}
-
-// Unnormalised length-N DFT with sign (+1 inverse, -1 forward) of the values
-// in `buf`.  Power-of-two N: `buf` holds the input in bit-reversed order
-// (inverse) or natural order (forward); the result is in natural order
-// (inverse) or bit-reversed order (forward).  Other N (Bluestein): `buf` has
-// room for M entries, holds the input in natural order in [0, N) and the
-// result in natural order in [0, N) for both signs.
-__device__ void ring_dft(cplx *buf, const DevRing &R, const RingParams &p, int sign) {
-  const int N = R.n / 2;
+// e^{2 pi i k / n}, 0 <= k <= n/2
+__device__ __forceinline__ cplx ring_root(const RingParams &p, const DevRing &R, int k) {
+  const int N = R.n >> 1;
   if (R.bluestein_m == 0) {
-    if (sign > 0) fft_dit(buf, N, p.twiddles, p.twlen, +1);
-    else fft_dif(buf, N, p.twiddles, p.twlen, -1);
-    return;
+    if (k == N) return {-1.0, 0.0};
+    const double2 t = p.twiddles[(int64_t)k * (p.twlen / R.n)];
+    return {t.x, t.y};
   }
-  const int M = R.bluestein_m;
-  // chirp with w^{-sign}: x_k w_k^{sign}, zero padded
-  for (int k = threadIdx.x; k < M; k += blockDim.x) {
-    cplx v = {0.0, 0.0};
-    if (k < N) {
-      cplx w = chirp(k, N);
-      if (sign < 0) w = cconj(w);
-      v = cmul(buf[k], w);
-    }
-    buf[k] = v;
+  const double2 t = p.aux[R.aux + N + k];
+  return {t.x, t.y};
+}
+
+// e^{i pi k^2 / N}, k < N (Bluestein rings)
+__device__ __forceinline__ cplx ring_chirp(const RingParams &p, const DevRing &R, int k) {
+  const double2 t = p.aux[R.aux + k];
+  return {t.x, t.y};
+}
+
+// Phase factor tables of one ring: lo[b] = e^{i b phi0}, hi[a] = e^{i 64 a phi0}
+// (all ones when phase shifting is off or phi0 = 0).
+__device__ void phase_tables(cplx *lo, cplx *hi, const RingParams &p, const DevRing &R) {
+  const bool on = p.phase_shifts && R.phi_num != 0;
+  for (int k = threadIdx.x; k < kPhaseLo + p.nphase_hi; k += blockDim.x) {
+    const long long m = k < kPhaseLo ? k : (long long)(k - kPhaseLo) * kPhaseLo;
+    const cplx v = on ? expi_pi(m * R.phi_num, R.phi_den) : cplx{1.0, 0.0};
+    if (k < kPhaseLo) lo[k] = v;
+    else hi[k - kPhaseLo] = v;
   }
-  __syncthreads();
-  fft_dif(buf, M, p.twiddles, p.twlen, -1);
-  // product with the filter spectrum (stored bit-reversed for sign +1; the
-  // sign -1 filter is its complex conjugate reflected: F'(p) = conj F(-p))
-  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + R.filter;
-  const int bits = ilog2(M);
-  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+}
+
+__device__ __forceinline__ cplx phase_at(const cplx *lo, const cplx *hi, int m) {
+  return cmul(hi[m >> 6], lo[m & (kPhaseLo - 1)]);
+}
+
+struct RingCta {
+  DevRing R;
+  int ring, map0, lg, nm;  // nm: maps of the group that exist
+  int n, N, M, bits, bitsM;
+  bool pow2;
+};
+
+__device__ __forceinline__ RingCta ring_cta(const RingParams &p, int task) {
+  RingCta c;
+  const DevRingTask T = p.tasks[task];
+  c.R = p.rings[T.ring];
+  c.ring = T.ring;
+  c.map0 = T.map0;
+  c.lg = T.lg;
+  c.nm = min(1 << T.lg, p.nmaps - T.map0);
+  c.n = c.R.n;
+  c.N = c.n >> 1;
+  c.pow2 = c.R.bluestein_m == 0;
+  c.M = c.pow2 ? c.N : c.R.bluestein_m;
+  c.bits = ilog2(c.N);
+  c.bitsM = ilog2(c.M);
+  return c;
+}
+
+// Cyclic convolution step of Bluestein's method on the chirped, zero-padded
+// buffer (natural order in, natural order out).
+__device__ void bluestein_convolve(cplx *buf, const RingCta &c, const RingParams &p, int sign) {
+  const int gm = (1 << c.lg) - 1, M = c.M;
+  fft_dif(buf, M, c.lg, p.twiddles, p.twlen, -1);
+  // filter spectrum, stored bit-reversed for sign +1; the sign -1 filter is
+  // its reflection F'(k) = F(-k), conjugated
+  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
+  for (int t = threadIdx.x; t < (M << c.lg); t += blockDim.x) {
+    const int g = t & gm, k = t >> c.lg;
     cplx f;
     if (sign > 0) {
       f = F[k];
     } else {
-      const unsigned natural = bitrev((unsigned)k, bits);
+      const unsigned natural = bitrev((unsigned)k, c.bitsM);
       const unsigned refl = (M - natural) & (M - 1);
-      f = cconj(F[bitrev(refl, bits)]);
+      f = cconj(F[bitrev(refl, c.bitsM)]);
     }
-    buf[k] = cmul(buf[k], f);
+    const int i = at(k, g, c.lg);
+    buf[i] = cmul(buf[i], f);
   }
   __syncthreads();
-  fft_dit(buf, M, p.twiddles, p.twlen, +1);
-  const double inv = 1.0 / (double)M;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    cplx w = chirp(k, N);
-    if (sign < 0) w = cconj(w);
-    buf[k] = cscale(cmul(buf[k], w), inv);
-  }
-  __syncthreads();
+  fft_dit(buf, M, c.lg, p.twiddles, p.twlen, +1);
 }
 
-__global__ void __launch_bounds__(kRingThreads) k_ring_synthesis(RingParams p) {
+// W[j] of one map (q row pointer `qg` at ring r, map g), aliasing sum in increasing m
+__device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mmax,
+                                          int64_t qstride, int64_t half, double sgn,
+                                          const cplx *plo, const cplx *phi) {
+  cplx acc = {0.0, 0.0};
+  for (int base = 0;; base += n) {
+    const int m1 = base + j;
+    if (m1 > mmax) break;
+    {
+      const cplx e = ld2(qg + m1 * qstride), o = ld2(qg + m1 * qstride + half);
+      const cplx t = {e.x + sgn * o.x, e.y + sgn * o.y};
+      acc = cadd(acc, cmul(t, phase_at(plo, phi, m1)));
+    }
+    const int m2 = base + n - j;
+    if (m2 <= mmax) {
+      const cplx e = ld2(qg + m2 * qstride), o = ld2(qg + m2 * qstride + half);
+      const cplx t = {e.x + sgn * o.x, e.y + sgn * o.y};
+      acc = cadd(acc, cconj(cmul(t, phase_at(plo, phi, m2))));
+    }
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kRingThreads, 3) k_ring_synthesis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
-  cplx *sm = reinterpret_cast<cplx *>(smem_d);
-  const int kmap = blockIdx.x, r = blockIdx.y;
-  const DevRing R = p.rings[r];
-  const int n = R.n, N = n / 2;
-  const int bits = ilog2(N);
-  const bool pow2 = R.bluestein_m == 0;
-  cplx *W = sm;            // N + 1
-  cplx *buf = sm + N + 1;  // N or M
-  const int64_t qstride_m = 2LL * p.ni * p.nvecs;  // q[(2m + odd) * ni * nvecs]
-  const int64_t qoff = (int64_t)r * p.nvecs + 2 * kmap;
-  const int64_t half = (int64_t)p.ni * p.nvecs;
+  const RingCta c = ring_cta(p, task0 + blockIdx.x);
+  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N;
+  cplx *buf = reinterpret_cast<cplx *>(smem_d);
+  cplx *plo = buf + ((int64_t)c.M << lg);
+  cplx *phi = plo + kPhaseLo;
+  phase_tables(plo, phi, p, c.R);
+  __syncthreads();
+  const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
+  const double *qbase = p.q + (int64_t)c.ring * p.nvecs + 2 * c.map0;
   for (int side = 0; side < 2; ++side) {
-    if (side == 1 && r == 0) break;  // the equator is written once
+    if (side == 1 && c.ring == 0) break;  // the equator is written once
     const double sgn = side ? -1.0 : 1.0;
-    for (int j = threadIdx.x; j <= N; j += blockDim.x) {
-      cplx acc = {0.0, 0.0};
-      for (int base = 0;; base += n) {
-        const int m1 = base + j;
-        if (m1 > p.mmax) break;
-        {
-          const double *qe = p.q + m1 * qstride_m + qoff;
-          const double *qo = qe + half;
-          cplx t = {qe[0] + sgn * qo[0], qe[1] + sgn * qo[1]};
-          acc = cadd(acc, cmul(t, phase(m1, R, p.phase_shifts)));
+    // Z[k] and Z[N - k] from W[k] and W[N - k]
+    const int npairs = (N >> 1) + 1;
+    for (int t = threadIdx.x; t < (npairs << lg); t += blockDim.x) {
+      const int g = t & gm, kk = t >> lg, kr = N - kk;
+      cplx Wa = {0.0, 0.0}, Wb = {0.0, 0.0};  // W[kk], W[N - kk]
+      if (g < c.nm) {
+        const double *qg = qbase + 2 * g;
+        Wa = alias_sum(qg, kk, n, p.mmax, qstride, half, sgn, plo, phi);
+        Wb = kr == kk ? Wa : alias_sum(qg, kr, n, p.mmax, qstride, half, sgn, plo, phi);
+      }
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int k = e ? kr : kk;
+        if (e && (kr == kk || kr == N)) break;
+        cplx Wk = e ? Wb : Wa, Wc = cconj(e ? Wa : Wb);
+        if (k == 0) {
+          Wk.y = 0.0;
+          Wc.y = 0.0;
         }
-        const int m2 = base + n - j;
-        if (m2 <= p.mmax) {
-          const double *qe = p.q + m2 * qstride_m + qoff;
-          const double *qo = qe + half;
-          cplx t = {qe[0] + sgn * qo[0], qe[1] + sgn * qo[1]};
-          acc = cadd(acc, cconj(cmul(t, phase(m2, R, p.phase_shifts))));
+        const cplx s = cadd(Wk, Wc), d = csub(Wk, Wc);
+        cplx Z = cadd(s, mul_i(cmul(ring_root(p, c.R, k), d)));
+        if (c.pow2) {
+          buf[at((int)bitrev((unsigned)k, c.bits), g, lg)] = Z;
+        } else {
+          buf[at(k, g, lg)] = cmul(Z, ring_chirp(p, c.R, k));
         }
       }
-      W[j] = acc;
     }
+    if (!c.pow2)
+      for (int t = threadIdx.x; t < ((c.M - N) << lg); t += blockDim.x)
+        buf[at(N + (t >> lg), t & gm, lg)] = {0.0, 0.0};
     __syncthreads();
-    for (int k = threadIdx.x; k < N; k += blockDim.x) {
-      cplx Wk = W[k], Wc = cconj(W[N - k]);
-      if (k == 0) {
-        Wk.y = 0.0;
-        Wc.y = 0.0;
-      }
-      const cplx s = cadd(Wk, Wc), d = csub(Wk, Wc);
-      const cplx Z = cadd(s, mul_i(cmul(unit_root(k, n), d)));
-      buf[pow2 ? bitrev((unsigned)k, bits) : k] = Z;
-    }
-    __syncthreads();
-    ring_dft(buf, R, p, +1);
-    const int64_t off = side ? R.off_south : R.off_north;
-    for (int s = threadIdx.x; s < N; s += blockDim.x) {
-      const cplx z = buf[s];
-      p.map[(off + 2 * s) * p.nmaps + kmap] = z.x;
-      p.map[(off + 2 * s + 1) * p.nmaps + kmap] = z.y;
+    if (c.pow2) fft_dit(buf, N, lg, p.twiddles, p.twlen, +1);
+    else bluestein_convolve(buf, c, p, +1);
+    const int64_t off = side ? c.R.off_south : c.R.off_north;
+    const double inv = c.pow2 ? 1.0 : 1.0 / (double)c.M;
+    double *out = p.map + off * p.nmaps + c.map0;
+    for (int t = threadIdx.x; t < (n << lg); t += blockDim.x) {
+      const int g = t & gm, pix = t >> lg, s = pix >> 1;
+      if (g >= c.nm) continue;
+      cplx z = buf[at(s, g, lg)];
+      if (!c.pow2) z = cscale(cmul(z, ring_chirp(p, c.R, s)), inv);
+      out[(int64_t)pix * p.nmaps + g] = (pix & 1) ? z.y : z.x;
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kRingThreads) k_ring_analysis(RingParams p) {
+__global__ void __launch_bounds__(kRingThreads, 3) k_ring_analysis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
-  cplx *sm = reinterpret_cast<cplx *>(smem_d);
-  const int kmap = blockIdx.x, r = blockIdx.y;
-  const DevRing R = p.rings[r];
-  const int n = R.n, N = n / 2;
-  const int bits = ilog2(N);
-  const bool pow2 = R.bluestein_m == 0;
-  cplx *F = sm;            // N + 1
-  cplx *buf = sm + N + 1;  // N or M
-  const int64_t qstride_m = 2LL * p.ni * p.nvecs;
-  const int64_t qoff = (int64_t)r * p.nvecs + 2 * kmap;
-  const int64_t half = (int64_t)p.ni * p.nvecs;
+  const RingCta c = ring_cta(p, task0 + blockIdx.x);
+  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N;
+  cplx *buf = reinterpret_cast<cplx *>(smem_d);
+  cplx *plo = buf + ((int64_t)c.M << lg);
+  cplx *phi = plo + kPhaseLo;
+  phase_tables(plo, phi, p, c.R);
+  const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
+  double *qbase = p.q_out + (int64_t)c.ring * p.nvecs + 2 * c.map0;
+  const double inv = c.pow2 ? 1.0 : 1.0 / (double)c.M;
   for (int side = 0; side < 2; ++side) {
-    if (side == 1 && r == 0) break;
-    const int64_t off = side ? R.off_south : R.off_north;
-    for (int s = threadIdx.x; s < N; s += blockDim.x)
-      buf[s] = {p.map_in[(off + 2 * s) * p.nmaps + kmap], p.map_in[(off + 2 * s + 1) * p.nmaps + kmap]};
+    if (side == 1 && c.ring == 0) break;
+    const int64_t off = side ? c.R.off_south : c.R.off_north;
+    const double *in = p.map_in + off * p.nmaps + c.map0;
+    for (int t = threadIdx.x; t < (N << lg); t += blockDim.x) {
+      const int g = t & gm, s = t >> lg;
+      cplx z = {0.0, 0.0};
+      if (g < c.nm) z = {in[(int64_t)(2 * s) * p.nmaps + g], in[(int64_t)(2 * s + 1) * p.nmaps + g]};
+      if (!c.pow2) z = cmul(z, cconj(ring_chirp(p, c.R, s)));
+      buf[at(s, g, lg)] = z;
+    }
+    if (!c.pow2)
+      for (int t = threadIdx.x; t < ((c.M - N) << lg); t += blockDim.x)
+        buf[at(N + (t >> lg), t & gm, lg)] = {0.0, 0.0};
     __syncthreads();
-    ring_dft(buf, R, p, -1);
-    // Z in natural order (Bluestein) or bit-reversed (power of two)
-    for (int k = threadIdx.x; k <= N; k += blockDim.x) {
-      const int k1 = k % N, k2 = (N - k) % N;
-      const cplx Zk = buf[pow2 ? bitrev((unsigned)k1, bits) : k1];
-      const cplx Zc = cconj(buf[pow2 ? bitrev((unsigned)k2, bits) : k2]);
+    if (c.pow2) fft_dif(buf, N, lg, p.twiddles, p.twlen, -1);
+    else bluestein_convolve(buf, c, p, -1);
+    // fold the spectrum F[k] (k <= N) into q~: g_m = F[m mod n] or its mirror
+    for (int t = threadIdx.x; t < ((p.mmax + 1) << lg); t += blockDim.x) {
+      const int g = t & gm, m = t >> lg;
+      if (g >= c.nm) continue;
+      const int jm = m % n;
+      const bool mirror = jm > N;
+      const int k = mirror ? n - jm : jm;
+      const int k1 = k == N ? 0 : k, k2 = k == 0 ? 0 : N - k;
+      cplx Zk, Zc;
+      if (c.pow2) {
+        Zk = buf[at((int)bitrev((unsigned)k1, c.bits), g, lg)];
+        Zc = buf[at((int)bitrev((unsigned)k2, c.bits), g, lg)];
+      } else {
+        Zk = cscale(cmul(buf[at(k1, g, lg)], cconj(ring_chirp(p, c.R, k1))), inv);
+        Zc = cscale(cmul(buf[at(k2, g, lg)], cconj(ring_chirp(p, c.R, k2))), inv);
+      }
+      Zc = cconj(Zc);
       const cplx E = cscale(cadd(Zk, Zc), 0.5);
       const cplx D = csub(Zk, Zc);
       const cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
-      F[k] = cadd(E, cmul(cconj(unit_root(k, n)), O));
-    }
-    __syncthreads();
-    for (int m = threadIdx.x; m <= p.mmax; m += blockDim.x) {
-      const int jm = m % n;
-      cplx g = jm <= N ? F[jm] : cconj(F[n - jm]);
-      g = cscale(cmul(g, cconj(phase(m, R, p.phase_shifts))), p.scale);
-      double *qe = p.q_out + m * qstride_m + qoff;
+      cplx F = cadd(E, cmul(cconj(ring_root(p, c.R, k)), O));
+      if (mirror) F = cconj(F);
+      const cplx gv = cscale(cmul(F, cconj(phase_at(plo, phi, m))), p.scale);
+      double *qe = qbase + m * qstride + 2 * g;
       double *qo = qe + half;
       if (side == 0) {
-        qe[0] = g.x; qe[1] = g.y;
-        qo[0] = g.x; qo[1] = g.y;
+        *reinterpret_cast<double2 *>(qe) = make_double2(gv.x, gv.y);
+        *reinterpret_cast<double2 *>(qo) = make_double2(gv.x, gv.y);
       } else {
-        qe[0] += g.x; qe[1] += g.y;
-        qo[0] -= g.x; qo[1] -= g.y;
+        const cplx e = ld2(qe), o = ld2(qo);
+        *reinterpret_cast<double2 *>(qe) = make_double2(e.x + gv.x, e.y + gv.y);
+        *reinterpret_cast<double2 *>(qo) = make_double2(o.x - gv.x, o.y - gv.y);
       }
     }
     __syncthreads();
   }
 }
 
-// Plan creation: twiddle table and the Bluestein filter spectra.
+// Plan creation: twiddle table, Bluestein chirp/root tables and filter spectra.
 __global__ void k_twiddles(double2 *tw, int twlen) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < twlen / 2; k += gridDim.x * blockDim.x) {
-    double s, c;
-    sincospi((double)(2 * k) / (double)twlen, &s, &c);
-    tw[k] = make_double2(c, s);
+    const cplx v = expi_pi(2LL * k, twlen);
+    tw[k] = make_double2(v.x, v.y);
+  }
+}
+
+__global__ void k_ring_aux(RingParams p) {
+  const DevRing R = p.rings[blockIdx.x];
+  if (R.bluestein_m == 0) return;
+  const int N = R.n / 2;
+  double2 *aux = reinterpret_cast<double2 *>(p.aux_out) + R.aux;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    const cplx v = expi_pi((long long)k * k, N);  // e^{i pi k^2 / N}
+    aux[k] = make_double2(v.x, v.y);
+  }
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) {
+    const cplx v = expi_pi(2LL * k, R.n);  // e^{2 pi i k / n}
+    aux[N + k] = make_double2(v.x, v.y);
   }
 }
 
@@ -335,41 +439,47 @@ __global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p
   // b_k = conj(e^{i pi k^2 / N}) for k in (-N, N), cyclically placed
   for (int k = threadIdx.x; k < M; k += blockDim.x) {
     cplx v = {0.0, 0.0};
-    if (k < N) v = cconj(chirp(k, N));
-    else if (k > M - N) v = cconj(chirp(M - k, N));
-    buf[k] = v;
+    if (k < N) v = cconj(expi_pi((long long)k * k, N));
+    else if (k > M - N) v = cconj(expi_pi((long long)(M - k) * (M - k), N));
+    buf[at(k, 0, 0)] = v;
   }
   __syncthreads();
-  fft_dif(buf, M, p.twiddles, p.twlen, -1);
+  fft_dif(buf, M, 0, p.twiddles, p.twlen, -1);
   cplx *F = reinterpret_cast<cplx *>(p.filters_out) + R.filter;
-  for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[k];
+  for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[at(k, 0, 0)];
+}
+
+template <class K>
+cudaError_t launch_classes(K kernel, const RingParams &prm, cudaStream_t st) {
+  const int smem_max = prm.smem0 > prm.smem1 ? prm.smem0 : prm.smem1;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
+  if (e != cudaSuccess) return e;
+  if (prm.ntasks0 > 0) {
+    kernel<<<prm.ntasks0, kRingThreads, prm.smem0, st>>>(prm, 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (prm.ntasks1 > 0) {
+    kernel<<<prm.ntasks1, kRingThreads, prm.smem1, st>>>(prm, prm.ntasks0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
 
-size_t ring_smem_bytes(int max_cplx) { return (size_t)max_cplx * sizeof(double) * 2; }
+int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi) {
+  return (int32_t)((buffer_cplx + kPhaseLo + nphase_hi) * 2 * sizeof(double));
+}
 
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
-  const size_t smem = ring_smem_bytes(prm.smem_cplx);
-  cudaError_t e = cudaFuncSetAttribute(k_ring_synthesis, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid(prm.nmaps, prm.ni);
-  k_ring_synthesis<<<grid, kRingThreads, smem, st>>>(prm);
-  return cudaGetLastError();
+  return launch_classes(k_ring_synthesis, prm, st);
 }
 
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
-  const size_t smem = ring_smem_bytes(prm.smem_cplx);
-  cudaError_t e = cudaFuncSetAttribute(k_ring_analysis, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  dim3 grid(prm.nmaps, prm.ni);
-  k_ring_analysis<<<grid, kRingThreads, smem, st>>>(prm);
-  return cudaGetLastError();
+  return launch_classes(k_ring_analysis, prm, st);
 }
 
-cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
+cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters, double *aux,
                               cudaStream_t st) {
   k_twiddles<<<64, 256, 0, st>>>(reinterpret_cast<double2 *>(twiddles), prm.twlen);
   cudaError_t e = cudaGetLastError();
@@ -377,8 +487,11 @@ cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *f
   RingParams q = prm;
   q.twiddles = reinterpret_cast<const double2 *>(twiddles);
   q.filters_out = filters;
-  const size_t smem = ring_smem_bytes(prm.max_bluestein_m);
-  e = cudaFuncSetAttribute(k_bluestein_filters, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  q.aux_out = aux;
+  k_ring_aux<<<prm.ni, 256, 0, st>>>(q);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int smem = prm.max_bluestein_m * 2 * (int)sizeof(double);
+  e = cudaFuncSetAttribute(k_bluestein_filters, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   k_bluestein_filters<<<prm.ni, kRingThreads, smem, st>>>(q);
   return cudaGetLastError();
