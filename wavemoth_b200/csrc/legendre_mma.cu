@@ -376,12 +376,18 @@ __global__ void __launch_bounds__(kThr, 1) k_m2a_residual(FastParams p) {
           }
         }
         {
-          // each thread stages one column (row of X) of the chunk
-          const int c = threadIdx.x;
-          const double *src = (c < nc) ? Xb + (int64_t)p.gcols[G.cols + c0 + c].row * p.nvecs + v0
-                                       : nullptr;
-#pragma unroll 8
-          for (int v = 0; v < VT; ++v) x_tile[c][v] = (src && v < vn) ? src[v] : 0.0;
+          // X rows of the chunk, warp-cooperative: LPC lanes per row, two
+          // vectors (16 bytes) per lane, so one load instruction covers
+          // whole rows
+          constexpr int LPC = VT / 2, RPI = 32 / LPC;
+          for (int cb = warp * RPI; cb < kPushCols; cb += 8 * RPI) {
+            const int c = cb + lane / LPC, v = 2 * (lane % LPC);
+            double2 val = make_double2(0.0, 0.0);
+            if (c < nc && v < vn)
+              val = *reinterpret_cast<const double2 *>(
+                  Xb + (int64_t)p.gcols[G.cols + c0 + c].row * p.nvecs + v0 + v);
+            *reinterpret_cast<double2 *>(&x_tile[c][v]) = val;
+          }
         }
         __syncthreads();
 #pragma unroll
