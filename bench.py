@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="split", choices=["split", "double"],
+                    help="split: sliced int8 tensor-core residual products (the plain FP64 path "
+                         "is timed beside it and is the error reference); double: plain FP64 only")
     ap.add_argument("--check", action="store_true",
                     help="also report the round-trip relative error of map 0 vs the FP64 oracle "
                          "at a reduced size (slow on CPU)")
@@ -285,7 +288,7 @@ def run_b200(a):
             dist.barrier()
 
     t0 = time.time()
-    T = Transform(path, a.nside, a.lmax, a.nmaps)
+    T = Transform(path, a.nside, a.lmax, a.nmaps, precision=a.precision)
     log("plan loaded in %.1f s" % (time.time() - t0))
     work = T.work()
     alm_h = synthetic_alm(a.lmax, a.nmaps, rank_seed(rank, a.nmaps))
@@ -296,6 +299,44 @@ def run_b200(a):
     def step(src):
         T.alm2map(src, out=maps)
         T.map2alm(maps, out=alm_out)
+
+    # plain FP64 path beside the split one: its rate and the split error
+    plain = None
+    if a.precision == "split":
+        TP = Transform(path, a.nside, a.lmax, a.nmaps, precision="double")
+        maps_p = torch.empty_like(maps)
+        alm_p = torch.empty_like(alm)
+
+        def step_p(src):
+            TP.alm2map(src, out=maps_p)
+            TP.map2alm(maps_p, out=alm_p)
+
+        for _ in range(a.warmup):
+            step_p(alm)
+        torch.cuda.synchronize()
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        for _ in range(a.steps):
+            step_p(alm)
+        p1.record()
+        torch.cuda.synchronize()
+        pms = 1e3 * reduce_max_seconds(p0.elapsed_time(p1) / 1e3, dist if world > 1 else None)
+        step(alm)
+        torch.cuda.synchronize()
+        T.device_status()
+
+        def maxrel(x, y):
+            return float((x - y).abs().max() / y.abs().max())
+
+        plain = {"value": job_rate(world, a.nmaps, a.steps, pms / 1e3), "unit": "maps/s",
+                 "ms_per_step": pms / a.steps,
+                 "max_rel_error_map": maxrel(maps, maps_p),
+                 "max_rel_error_alm_round_trip": maxrel(alm_out, alm_p),
+                 "error_definition": "max |split - plain FP64| / max |plain FP64| over the alm2map "
+                                     "output and over the alm2map+map2alm output, same inputs"}
+        TP.close()
+        del maps_p, alm_p
 
     for _ in range(a.warmup):
         step(alm)
@@ -393,7 +434,11 @@ def run_b200(a):
         "config": {"workload": "alm2map+map2alm round trip, nside %d, lmax=mmax %d, %d maps per GPU"
                                % (a.nside, a.lmax, a.nmaps),
                    "nside": a.nside, "lmax": a.lmax, "nmaps_per_gpu": a.nmaps,
-                   "precision": "plain FP64", "plan": {"eps": a.eps, "chunk": a.chunk,
+                   "precision": ("split: residual products as sliced int8 tcgen05 GEMMs (6 slices, "
+                                 "products i+j<=6), FP64 recurrence/levels/rings"
+                                 if a.precision == "split" else "plain FP64"),
+                   "plain_fp64": plain,
+                   "plan": {"eps": a.eps, "chunk": a.chunk,
                                                        "memop_cost": a.memop},
                    "parallelism": "replicas (maps sharded per GPU)" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (alm %.2f GB, maps %.2f GB per GPU)"

@@ -19,6 +19,9 @@ extern "C" {
 
 /* additive plan flags */
 #define WAVEMOTH_DEVICE_POINTERS 0x100   /* input/output given at plan time are device pointers */
+#define WAVEMOTH_PRECISION_SPLIT 0x200   /* residual products of depth-0/1 matrices as sliced int8
+                                            tensor-core GEMMs re-summed in FP64 (Ozaki scheme);
+                                            the recurrence, seeds and scales stay FP64 */
 
 /* status codes */
 #define WAVEMOTH_OK 0
@@ -33,6 +36,13 @@ const char *wavemoth_last_error(void);
 
 /* Status of the last call made on the plan (WAVEMOTH_OK or an error code). */
 int wavemoth_plan_status(wavemoth_plan plan);
+
+/* Waits for `stream` (NULL: the default stream) and returns the plan's
+   device status word as a status code (WAVEMOTH_ERR_DEVICE if a kernel
+   recorded an expired bounded wait or a bad table entry), clearing it.
+   New; device-pointer executes are asynchronous and report kernel-side
+   errors only through this call. */
+int wavemoth_plan_device_status(wavemoth_plan plan, void *stream);
 
 /* map2alm plan: the analysis direction, defined as (4 pi / Npix) times the
    adjoint of alm2map (a_lm = 4pi/Npix sum_p f_p lambda_lm(theta_p)

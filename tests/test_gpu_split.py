@@ -1,0 +1,80 @@
+"""Split-precision (sliced int8 tensor-core) residual products against the
+plain FP64 path on the same plans and inputs.
+
+Tolerance: the maximum absolute difference over the output, relative to the
+maximum magnitude of the FP64 result, at most 1e-9 (the split-precision
+acceptance bound); the FP64 path itself is pinned to the reference at 1e-10
+in test_gpu_parity.py.  Plans cover depth-0 and depth-1 butterfly trees,
+1, 5 and 40 maps (80 vectors: two passes of 64), both directions.
+"""
+import numpy as np
+import pytest
+
+from oracle import sht as osht
+from wavemoth_b200 import lib as wlib
+
+from .plans import plan_file
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [
+    # nside, lmax, chunk, eps, memop
+    (8, 16, 8, 1e-10, 1.0),
+    (16, 32, 8, 1e-10, 1e-10),
+    (32, 64, 16, 1e-10, 20.0),
+    (64, 128, 64, 1e-10, 20.0),
+]
+
+
+def maxrel(got, want):
+    return float(np.abs(got - want).max() / np.abs(want).max())
+
+
+def _run(path, nside, lmax, inp, direction, precision):
+    if direction == "alm2map":
+        out = np.zeros((12 * nside * nside, inp.shape[1]))
+    else:
+        out = np.zeros(((lmax + 1) * (lmax + 2) // 2, inp.shape[1]), np.complex128)
+    p = wlib.ShtPlan(nside, lmax, lmax, np.ascontiguousarray(inp), out, "mmajor",
+                     matrix_data_filename=path, direction=direction, precision=precision)
+    res = p.execute().copy()
+    p.close()
+    return res
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+@pytest.mark.parametrize("nmaps", [1, 5, 40])
+def test_split_alm2map(cfg, nmaps):
+    nside, lmax, chunk, eps, memop = cfg
+    path = plan_file(nside, lmax, chunk, eps, memop)
+    alm = osht.random_alm(lmax, nmaps, seed=300 + nmaps)
+    ref = _run(path, nside, lmax, alm, "alm2map", "double")
+    got = _run(path, nside, lmax, alm, "alm2map", "split")
+    assert maxrel(got, ref) <= 1e-9
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+@pytest.mark.parametrize("nmaps", [1, 40])
+def test_split_map2alm(cfg, nmaps):
+    nside, lmax, chunk, eps, memop = cfg
+    path = plan_file(nside, lmax, chunk, eps, memop)
+    maps = np.random.default_rng(400 + nmaps).standard_normal((12 * nside * nside, nmaps))
+    ref = _run(path, nside, lmax, maps, "map2alm", "double")
+    got = _run(path, nside, lmax, maps, "map2alm", "split")
+    assert maxrel(got, ref) <= 1e-9
+
+
+def test_split_against_oracle_and_status():
+    """Split alm2map against the oracle's butterfly transform; the device
+    status word stays clear."""
+    import torch
+    from wavemoth_b200.sht import Transform
+    nside, lmax = 32, 64
+    path = plan_file(nside, lmax, 16, 1e-10, 20.0)
+    alm = osht.random_alm(lmax, 3, seed=17)
+    T = Transform(path, nside, lmax, 3, precision="split")
+    got = T.alm2map(torch.from_numpy(alm).cuda()).cpu().numpy()
+    T.device_status()
+    want = osht.alm2map_butterfly(osht.Rev1File(path), alm, lmax)
+    assert maxrel(got, want) <= 1e-9
+    T.close()

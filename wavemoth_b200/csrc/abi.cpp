@@ -85,6 +85,14 @@ struct _wavemoth_plan {
   wm::DevRootUnit *d_roots = nullptr;
   double *d_seeds = nullptr;
   double *d_xbuf = nullptr;
+  // split-precision residual path
+  bool split = false;
+  wm::DevSplitGroup *d_sgroups = nullptr;
+  wm::DevSplitTileA *d_stiles_a = nullptr;
+  wm::DevSplitTileB *d_stiles_b = nullptr;
+  double2 *d_col_scale = nullptr, *d_row_scale = nullptr, *d_vec_scale = nullptr;
+  int8_t *d_planes = nullptr;
+  int32_t *d_status = nullptr;
   wm::DevRing *d_rings = nullptr;
   wm::DevRingTask *d_ring_tasks = nullptr;
   double *d_twiddles = nullptr, *d_filters = nullptr, *d_ring_aux = nullptr;
@@ -268,6 +276,34 @@ wm::FastParams fast_params(wavemoth_plan P) {
   return f;
 }
 
+wm::SplitParams split_params(wavemoth_plan P) {
+  const auto &G = P->prog;
+  wm::SplitParams s{};
+  s.mats = P->d_mats;
+  s.f64 = P->d_f64;
+  s.groups = P->d_groups;
+  s.gcols = P->d_gcols;
+  s.sgroups = P->d_sgroups;
+  s.tiles_a = P->d_stiles_a;
+  s.tiles_b = P->d_stiles_b;
+  s.ngroups = (int32_t)G.groups.size();
+  s.ngcols = (int64_t)G.gcols.size();
+  s.ntiles_a = (int32_t)G.stiles_a.size();
+  s.ntiles_b = (int32_t)G.stiles_b.size();
+  s.seeds = P->d_seeds;
+  s.col_scale = P->d_col_scale;
+  s.row_scale = P->d_row_scale;
+  s.vec_scale = P->d_vec_scale;
+  s.planes = P->d_planes;
+  s.nrowscale = G.split_rows;
+  s.lmax = P->lmax;
+  s.nvecs = P->nvecs;
+  s.ni = P->ni;
+  s.xbuf = P->d_xbuf;
+  s.status = P->d_status;
+  return s;
+}
+
 wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps, double *input,
                         double *output, int ordering, unsigned flags, const char *resource_filename) {
   if (nmaps <= 0 || lmax < 0 || mmax != lmax || ordering != WAVEMOTH_MMAJOR) {
@@ -377,6 +413,19 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
     rc = rc ? rc : A.alloc(&P->d_ring_aux, (size_t)std::max<int64_t>(2 * RT.aux_cplx, 2),
                            "Bluestein chirps");
   }
+  P->split = (flags & WAVEMOTH_PRECISION_SPLIT) != 0;
+  if (P->split) {
+    rc = rc ? rc : upload(A, &P->d_sgroups, G.sgroups, "split groups");
+    rc = rc ? rc : upload(A, &P->d_stiles_a, G.stiles_a, "split alm2map tiles");
+    rc = rc ? rc : upload(A, &P->d_stiles_b, G.stiles_b, "split map2alm tiles");
+    rc = rc ? rc : A.alloc(&P->d_col_scale, (size_t)std::max<int64_t>((int64_t)G.gcols.size(), 1), "column scales");
+    rc = rc ? rc : A.alloc(&P->d_row_scale, (size_t)std::max<int64_t>(G.split_rows, 1), "row scales");
+    rc = rc ? rc : A.alloc(&P->d_vec_scale, (size_t)std::max<size_t>(G.groups.size(), 1) * wm::kSplitN,
+                           "vector scales");
+    rc = rc ? rc : A.alloc(&P->d_planes, (size_t)std::max<int64_t>(G.split_chunks, 1) * wm::kSplitPlane,
+                           "operand slices");
+  }
+  rc = rc ? rc : A.alloc(&P->d_status, 1, "status word");
   rc = rc ? rc : A.alloc(&P->d_counter, 1, "counter");
   rc = rc ? rc : A.alloc(&P->d_q, (size_t)2 * (mmax + 1) * P->ni * P->nvecs, "q buffer");
   rc = rc ? rc : A.alloc(&P->d_scratch, (size_t)P->grid * P->slot_stride, "butterfly scratch");
@@ -397,6 +446,24 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
     fp.seeds_out = P->d_seeds;
     rc = cuda_check(wm::launch_seeds(fp, P->stream), "seed kernel launch");
     if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "seed kernel");
+  }
+  if (!rc) rc = cuda_check(cudaMemsetAsync(P->d_status, 0, sizeof(int32_t), P->stream), "status reset");
+  if (!rc && P->split && !G.gcols.empty()) {
+    // per-column and per-row maxima of P (scratch freed after use)
+    unsigned long long *colmax = nullptr, *rowmax = nullptr;
+    const size_t nc = G.gcols.size(), nr = (size_t)std::max<int64_t>(G.split_rows, 1);
+    rc = cuda_check(cudaMalloc(&colmax, nc * sizeof(unsigned long long)), "scale scratch");
+    if (!rc) rc = cuda_check(cudaMalloc(&rowmax, nr * sizeof(unsigned long long)), "scale scratch");
+    if (!rc) rc = cuda_check(cudaMemsetAsync(rowmax, 0, nr * sizeof(unsigned long long), P->stream), "scale scratch");
+    if (!rc) {
+      wm::SplitParams sp = split_params(P);
+      sp.colmax = colmax;
+      sp.rowmax = rowmax;
+      rc = cuda_check(wm::launch_split_scales(sp, P->stream), "split scale launch");
+      if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "split scales");
+    }
+    cudaFree(colmax);
+    cudaFree(rowmax);
   }
   if (rc) {
     delete P;
@@ -497,6 +564,29 @@ int fast_grid(wavemoth_plan P, int units) {
   return std::max(1, std::min(units, 4 * P->sm_count));
 }
 
+// Split-precision residual products, kSplitN vectors per pass: operand
+// slices of the pass, then the tensor-core GEMM of every group tile.
+int run_split(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_out, const double *q_in,
+              double *q_out, cudaStream_t st) {
+  const auto &G = P->prog;
+  if (G.groups.empty()) return 0;
+  wm::SplitParams s = split_params(P);
+  s.alm_in = alm_in;
+  s.alm_out = alm_out;
+  s.q_in = q_in;
+  s.q = q_out;
+  const int nt = alm2map ? s.ntiles_a : s.ntiles_b;
+  for (int v0 = 0; v0 < P->nvecs; v0 += wm::kSplitN) {
+    s.v0 = v0;
+    int rc = cuda_check(wm::launch_split(alm2map ? 0 : 2, s, std::min((int)G.groups.size(), 8 * P->sm_count), st),
+                        "operand slice launch");
+    if (!rc && nt)
+      rc = cuda_check(wm::launch_split(alm2map ? 1 : 3, s, std::min(nt, P->sm_count), st), "split GEMM launch");
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_out,
                  const double *q_in, double *q_out, cudaStream_t st) {
   const auto &G = P->prog;
@@ -509,11 +599,13 @@ int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *al
   f.q = q_out;
   const int nta = (int)G.tiles_a.size(), ntb = (int)G.tiles_b.size(), nr = (int)G.roots.size();
   if (alm2map) {
-    if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
+    if (P->split) rc = run_split(P, true, alm_in, alm_out, q_in, q_out, st);
+    else if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
     if (!rc && nr) rc = cuda_check(wm::launch_fast(1, f, fast_grid(P, nr), st), "alm2map level launch");
   } else {
     if (nr) rc = cuda_check(wm::launch_fast(2, f, fast_grid(P, nr), st), "map2alm level launch");
-    if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
+    if (P->split) rc = rc ? rc : run_split(P, false, alm_in, alm_out, q_in, q_out, st);
+    else if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
   }
   if (!rc && P->nslow > 0) {
     wm::LegendreParams p = legendre_params(P);
@@ -554,6 +646,17 @@ int run_map2alm(wavemoth_plan P, const double *map, double *alm, cudaStream_t st
   return run_legendre(P, false, nullptr, alm, P->d_q, nullptr, st);
 }
 
+// Reads (and clears) the device status word; the stream must be idle.
+int device_status(wavemoth_plan P) {
+  int32_t st = 0;
+  int rc = cuda_check(cudaMemcpy(&st, P->d_status, sizeof(st), cudaMemcpyDeviceToHost), "status read");
+  if (rc) return rc;
+  if (st == 0) return 0;
+  cudaMemset(P->d_status, 0, sizeof(st));
+  return set_error(WAVEMOTH_ERR_DEVICE, st == wm::kStatusTimeout ? "a kernel's bounded wait expired"
+                                                                 : "a kernel reported a bad program table");
+}
+
 int finish(wavemoth_plan P, int rc) {
   P->status = rc;
   return rc;
@@ -589,6 +692,7 @@ int host_execute(wavemoth_plan P) {
                       "alm download");
   }
   if (!rc) rc = cuda_check(cudaStreamSynchronize(st), "execute");
+  if (!rc) rc = device_status(P);
   return rc;
 }
 
@@ -631,6 +735,12 @@ void wavemoth_execute(wavemoth_plan plan) {
 }
 
 int wavemoth_plan_status(wavemoth_plan plan) { return plan ? plan->status : WAVEMOTH_ERR_ARG; }
+
+int wavemoth_plan_device_status(wavemoth_plan plan, void *stream) {
+  if (!plan) return set_error(WAVEMOTH_ERR_ARG, "NULL plan");
+  if (int rc = cuda_check(cudaStreamSynchronize((cudaStream_t)stream), "device status")) return rc;
+  return finish(plan, device_status(plan));
+}
 
 int64_t wavemoth_get_legendre_flops(wavemoth_plan plan, int m, int odd) {
   if (!plan || m < 0 || m > plan->mmax || odd < 0 || odd > 1) return -1;

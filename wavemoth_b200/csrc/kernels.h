@@ -58,6 +58,41 @@ cudaError_t launch_fast(int which, const FastParams &prm, int grid, cudaStream_t
 cudaError_t launch_seeds(const FastParams &prm, cudaStream_t st);
 int fast_vector_tiles(int nvecs);
 
+// Split-precision residual path (legendre_split.cu).
+struct SplitParams {
+  const DevMatrix *mats;
+  const double *f64;
+  const DevGroup *groups;
+  const DevGCol *gcols;
+  const DevSplitGroup *sgroups;
+  const DevSplitTileA *tiles_a;
+  const DevSplitTileB *tiles_b;
+  int32_t ngroups;
+  int64_t ngcols;
+  int32_t ntiles_a, ntiles_b;
+  const double *seeds;            // recurrence seeds every kSeedRows rows (k_seeds)
+  double2 *col_scale;             // per group column: (2^e, 2^-e) of P (alm2map)
+  double2 *row_scale;             // per group row: (2^e, 2^-e) of P (map2alm)
+  double2 *vec_scale;             // per group x kSplitN: scales of the alm / X operand
+  int8_t *planes;                 // sliced alm / X operand chunks
+  unsigned long long *colmax;     // plan creation: max |P| bits per column
+  unsigned long long *rowmax;     // plan creation: max |P| bits per row
+  int64_t nrowscale;
+  int32_t lmax, nvecs, ni;
+  int32_t v0;                     // first vector of this pass (kSplitN per pass)
+  const double *alm_in;
+  double *alm_out;
+  const double *q_in;             // map2alm: q~
+  double *q;                      // alm2map: q
+  double *xbuf;
+  int32_t *status;                // device status word (kStatus*)
+};
+
+// which: 0 alm operand slices, 1 alm2map residual, 2 X operand slices, 3 map2alm residual
+cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream_t st);
+// Plan creation: P scales of both directions.
+cudaError_t launch_split_scales(const SplitParams &prm, cudaStream_t st);
+
 int legendre_threads();
 cudaError_t launch_legendre(bool alm2map, const LegendreParams &prm, int grid, cudaStream_t st);
 

@@ -17,10 +17,10 @@
 // (g, t); B (4x8, col) element (t, g); C/D (8x8) elements (g, 2t) and (g, 2t+1).
 //
 // Every output element has one writer and a fixed summation order, so results
-// are bitwise reproducible.  map2alm rows of one group are split into chunks
-// of kPushRows rows that start from recurrence seeds stored at the chunk
-// boundaries (computed once per plan by k_seeds), so no cross-CTA reduction
-// is needed.
+// are bitwise reproducible.  map2alm rows of one group are split into units
+// of kPushRows rows that start from recurrence seeds stored every kSeedRows
+// rows (computed once per plan by k_seeds), so no cross-CTA reduction is
+// needed.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -442,7 +442,7 @@ __global__ void k_seeds(FastParams p) {
   double a = p.f64[C.data + C.nx], b = p.f64[C.data + 2 * C.nx];  // P[row], P[row + 1]
   int row = C.start;
   for (int j = 0; j < G.nchunks; ++j) {
-    const int target = max(j * kPushRows, C.start);
+    const int target = max(j * kSeedRows, C.start);
     if (target >= G.nrows) break;
     while (row < target) {
       // P[row + 2] exists only inside the group's rows

@@ -90,7 +90,7 @@ struct DevGroup {
   int32_t ncols;      // skeleton columns of all the group's blocks
   int64_t cols;       // index of the group's first DevGCol
   int64_t seeds;      // index (in doubles) of the group's seeds: ncols x nchunks x 2
-  int32_t nchunks;    // row chunks of kPushRows rows
+  int32_t nchunks;    // seed chunks of kSeedRows rows
   int32_t in_q;       // 1: the columns are rows of q (depth 0); 0: rows of the X buffer
 };
 
@@ -110,14 +110,43 @@ struct DevTileA {     // alm2map residual unit: <= 64 consecutive group columns
 };
 
 struct DevTileB {     // map2alm residual unit: <= kPushRows consecutive group rows
-  int32_t group, row0, nrows, chunk;
+  int32_t group, row0, nrows, chunk;   // chunk: seed chunk of row0
 };
 
 struct DevRootUnit {  // depth-1 level unit: one root's interpolation pair
   int32_t matrix, pair;
 };
 
-constexpr int kPushRows = 32;
+constexpr int kPushRows = 32;   // rows of a map2alm residual unit (FP64 tensor-core path)
+constexpr int kSeedRows = 16;   // spacing of the recurrence seeds (P at rows s, s + 1)
+
+// ---- split-precision residual path (sliced int8 operands, tcgen05) ----
+//
+// The residual GEMMs of the row groups above, with both operands cut into
+// kSplitSlices signed 7-bit slices under power-of-two scales (per skeleton
+// column for alm2map, per matrix row for map2alm, per group and vector for
+// the alm / X operand) and accumulated exactly in int32 on the tensor cores.
+constexpr int kSplitSlices = 6;
+constexpr int kSplitK = 64;       // K chunk (rows for alm2map, columns for map2alm)
+constexpr int kSplitM = 128;      // M tile (columns for alm2map, rows for map2alm)
+constexpr int kSplitN = 64;       // vectors per pass
+constexpr int kSplitPlane = kSplitSlices * kSplitN * kSplitK;  // bytes of one operand chunk
+
+struct DevSplitGroup {
+  int64_t apl;        // first alm-operand chunk (alm2map): ceil(nrows / kSplitK) chunks
+  int64_t xpl;        // first X-operand chunk (map2alm): ceil(ncols / kSplitK) chunks
+  int64_t rowoff;     // first entry of the group's row scales
+  int32_t nrchunks;
+  int32_t ncchunks;
+};
+
+struct DevSplitTileA {  // alm2map: <= kSplitM columns of a group, K chunks from kc0
+  int32_t group, col0, ncols, kc0;
+};
+
+struct DevSplitTileB {  // map2alm: <= kSplitM rows of a group, all its columns
+  int32_t group, row0, nrows, pad;
+};
 
 // Per ring pair (ring number r from the equator).
 struct DevRing {

@@ -446,6 +446,46 @@ namespace wm {
 // all rows) and depth 1 (every root a (T, B) pair over two leaves, T blocks
 // on rows [0, nk/2), B blocks on [nk/2, nk) -- butterfly.pyx:570-573) are
 // taken; anything else stays with the generic kernels.
+// Split-precision residual tables: operand chunk offsets per group and the
+// M tiles of both directions, largest K extent first.
+static void build_split_tables(HostProgram &P) {
+  P.sgroups.clear();
+  P.stiles_a.clear();
+  P.stiles_b.clear();
+  int64_t apl = 0, xpl = 0, rows = 0;
+  std::vector<std::pair<int32_t, DevSplitTileA>> ta;
+  std::vector<std::pair<int32_t, DevSplitTileB>> tb;
+  for (int32_t gi = 0; gi < (int32_t)P.groups.size(); ++gi) {
+    const DevGroup &G = P.groups[gi];
+    DevSplitGroup S{};
+    S.nrchunks = (G.nrows + kSplitK - 1) / kSplitK;
+    S.ncchunks = (G.ncols + kSplitK - 1) / kSplitK;
+    S.apl = apl;
+    S.xpl = xpl;
+    S.rowoff = rows;
+    apl += S.nrchunks;
+    xpl += S.ncchunks;
+    rows += G.nrows;
+    P.sgroups.push_back(S);
+    for (int32_t c0 = 0; c0 < G.ncols; c0 += kSplitM) {
+      DevSplitTileA T{gi, c0, std::min(kSplitM, G.ncols - c0), G.nrows};
+      for (int32_t c = c0; c < c0 + T.ncols; ++c)
+        T.kc0 = std::min(T.kc0, P.gcols[G.cols + c].start);
+      T.kc0 /= kSplitK;
+      if (T.kc0 < S.nrchunks) ta.push_back({S.nrchunks - T.kc0, T});
+    }
+    if (S.ncchunks > 0)
+      for (int32_t r0 = 0; r0 < G.nrows; r0 += kSplitM)
+        tb.push_back({S.ncchunks, DevSplitTileB{gi, r0, std::min(kSplitM, G.nrows - r0), 0}});
+  }
+  std::stable_sort(ta.begin(), ta.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+  std::stable_sort(tb.begin(), tb.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+  for (auto &t : ta) P.stiles_a.push_back(t.second);
+  for (auto &t : tb) P.stiles_b.push_back(t.second);
+  P.split_chunks = std::max(apl, xpl);
+  P.split_rows = rows;
+}
+
 bool build_fast_path(HostProgram &P, std::string &err) {
   P.groups.clear();
   P.gcols.clear();
@@ -537,7 +577,7 @@ bool build_fast_path(HostProgram &P, std::string &err) {
         }
       }
       G.ncols = (int32_t)(P.gcols.size() - G.cols);
-      G.nchunks = (G.nrows + kPushRows - 1) / kPushRows;
+      G.nchunks = (G.nrows + kSeedRows - 1) / kSeedRows;
       G.seeds = P.nseeds;
       P.nseeds += 2LL * G.ncols * G.nchunks;
       const int32_t gi = (int32_t)P.groups.size();
@@ -551,10 +591,11 @@ bool build_fast_path(HostProgram &P, std::string &err) {
         T.kstart &= ~3;
         P.tiles_a.push_back(T);
       }
-      for (int32_t j = 0; j < G.nchunks; ++j)
-        P.tiles_b.push_back(DevTileB{gi, j * kPushRows, std::min(kPushRows, G.nrows - j * kPushRows), j});
+      for (int32_t r0 = 0; r0 < G.nrows; r0 += kPushRows)
+        P.tiles_b.push_back(DevTileB{gi, r0, std::min(kPushRows, G.nrows - r0), r0 / kSeedRows});
     }
   }
+  build_split_tables(P);
   return true;
 }
 

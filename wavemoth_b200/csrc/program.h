@@ -30,6 +30,12 @@ struct HostProgram {
   int64_t xrows = 0;                    // rows of the X buffer
   int32_t max_root_k = 0;               // largest kT + kB of a depth-1 root
   int32_t max_root_n = 0;               // largest n of a depth-1 root
+  // split-precision residual tables (see plan.h)
+  std::vector<DevSplitGroup> sgroups;   // one per group
+  std::vector<DevSplitTileA> stiles_a;
+  std::vector<DevSplitTileB> stiles_b;
+  int64_t split_chunks = 0;             // operand chunks of the larger direction
+  int64_t split_rows = 0;               // row scales (sum of group rows)
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)

@@ -16,6 +16,7 @@ WAVEMOTH_ESTIMATE = 0x0
 WAVEMOTH_MEASURE = 0x1
 WAVEMOTH_NO_RESOURCE_COPY = 0x10
 WAVEMOTH_DEVICE_POINTERS = 0x100
+WAVEMOTH_PRECISION_SPLIT = 0x200
 
 _configured = False
 
@@ -57,11 +58,13 @@ class ShtPlan:
     """
 
     def __init__(self, Nside, lmax, mmax, input, output, ordering, phase_shifts=True,
-                 matrix_data_filename=None, nthreads=1, direction="alm2map"):
+                 matrix_data_filename=None, nthreads=1, direction="alm2map", precision="double"):
         if ordering != "mmajor":
             raise ValueError("Invalid ordering: %s" % ordering)
         if direction not in ("alm2map", "map2alm"):
             raise ValueError("Invalid direction: %s" % direction)
+        if precision not in ("double", "split"):
+            raise ValueError("Invalid precision: %s" % precision)
         alm, maps = (input, output) if direction == "alm2map" else (output, input)
         if not (isinstance(alm, np.ndarray) and alm.dtype == np.complex128 and alm.ndim == 2
                 and alm.flags.c_contiguous):
@@ -84,7 +87,8 @@ class ShtPlan:
         fn = (_lib().wavemoth_plan_to_healpix if direction == "alm2map"
               else _lib().wavemoth_plan_from_healpix)
         self._plan = fn(Nside, lmax, mmax, self.nmaps, nthreads,
-                        input.ctypes.data, output.ctypes.data, WAVEMOTH_MMAJOR, WAVEMOTH_ESTIMATE,
+                        input.ctypes.data, output.ctypes.data, WAVEMOTH_MMAJOR,
+                        WAVEMOTH_ESTIMATE | (WAVEMOTH_PRECISION_SPLIT if precision == "split" else 0),
                         None if matrix_data_filename is None else os.fsencode(matrix_data_filename))
         if not self._plan:
             raise WavemothError("Plan creation failed: " + last_error())

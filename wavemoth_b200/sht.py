@@ -10,23 +10,29 @@ import os
 import torch
 
 from . import _native
-from .lib import WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WavemothError, last_error
+from .lib import (WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WAVEMOTH_PRECISION_SPLIT, WavemothError,
+                  last_error)
 
 
 class Transform:
     """Both directions share one device plan (the compiled butterfly program
-    serves A^T for alm2map and A for map2alm)."""
+    serves A^T for alm2map and A for map2alm).  precision='split' runs the
+    residual products as sliced int8 tensor-core GEMMs re-summed in FP64."""
 
-    def __init__(self, resource_file, nside, lmax, nmaps=1):
+    def __init__(self, resource_file, nside, lmax, nmaps=1, precision="double"):
         if not torch.cuda.is_available():
             raise RuntimeError("wavemoth_b200.Transform needs a CUDA device")
         self.nside, self.lmax, self.nmaps = nside, lmax, nmaps
         self.npix = 12 * nside * nside
         self.nalm = (lmax + 1) * (lmax + 2) // 2
         self.resource_file = resource_file
+        if precision not in ("double", "split"):
+            raise ValueError("precision must be 'double' or 'split'")
+        self.precision = precision
+        flags = WAVEMOTH_DEVICE_POINTERS | (WAVEMOTH_PRECISION_SPLIT if precision == "split" else 0)
         lib = _native.lib()
         p = lib.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR,
-                                         WAVEMOTH_DEVICE_POINTERS, os.fsencode(resource_file))
+                                         flags, os.fsencode(resource_file))
         if not p:
             raise WavemothError("plan creation failed: " + last_error())
         self._plan = p
@@ -66,6 +72,13 @@ class Transform:
         if rc != 0:
             raise WavemothError("map2alm failed (%d): %s" % (rc, last_error()))
         return out
+
+    def device_status(self):
+        """Waits for torch's current stream and raises if a kernel recorded an
+        error in the plan's device status word (e.g. an expired bounded wait)."""
+        rc = _native.lib().wavemoth_plan_device_status(self._plan, self._stream())
+        if rc != 0:
+            raise WavemothError("device status (%d): %s" % (rc, last_error()))
 
     @property
     def plan_handle(self):
