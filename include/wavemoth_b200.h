@@ -115,7 +115,11 @@ int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out);
    out[0] Legendre flops (2 per multiply-add, 5 per recurrence step),
    out[1] compressed-matrix bytes read, out[2] alm + q bytes of one Legendre
    launch, out[3] q + map bytes of one ring launch, out[4..6] interpolation /
-   recurrence / dense residual element counts, out[7] Legendre grid size. */
+   recurrence / dense residual element counts, out[7] Legendre grid size,
+   and for the split-precision residual products (out needs 12 entries):
+   out[8] / out[9] elements of P generated by the alm2map / map2alm tiles
+   per pass of 64 vectors (zero padding of the tiles included), out[10] /
+   out[11] int8 tensor-core operations of one alm2map / map2alm launch. */
 int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out);
 
 /* Parses and validates a rev1 file for (Nside, lmax) exactly as plan

@@ -875,6 +875,19 @@ int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out) {
   out[5] = (double)G.rec_elems;
   out[6] = (double)G.dense_elems;
   out[7] = (double)plan->grid;
+  // split path: 64-row (or 64-column) K chunks of 128-row M tiles; per K
+  // step of 32, nine MMAs with N summing to 1664 (six slices, i + j <= 6)
+  double ea = 0.0, eb = 0.0;
+  for (const auto &T : G.stiles_a) ea += (double)(G.sgroups[T.group].nrchunks - T.kc0);
+  for (const auto &T : G.stiles_b) eb += (double)G.sgroups[T.group].ncchunks;
+  ea *= (double)wm::kSplitM * wm::kSplitK;
+  eb *= (double)wm::kSplitM * wm::kSplitK;
+  const double passes = (double)((2 * nmaps + wm::kSplitN - 1) / wm::kSplitN);
+  const double ops_per_elem = 2.0 * 1664.0;  // per element of P (M x K), all slice windows
+  out[8] = ea;
+  out[9] = eb;
+  out[10] = ea * ops_per_elem * passes;
+  out[11] = eb * ops_per_elem * passes;
   return 0;
 }
 

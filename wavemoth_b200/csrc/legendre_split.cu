@@ -378,19 +378,38 @@ __device__ __forceinline__ double recombine(const int32_t (&d)[kSplitDiag][8], i
 
 // P at rows r0 .. r0 + 15 of group column c (zero outside [C.start, nrows)):
 // dense values, or the recurrence from the seeds (P at s0 = max(r0, start)
-// and s0 + 1) stored for the seed chunk of r0.
-__device__ __forceinline__ void column_segment(const SplitParams &p, const DevGroup &G, const DevGCol &C,
+// and s0 + 1) stored for the seed chunk of r0.  Returns false when the
+// segment lies entirely outside the column's active rows (all zeros).
+__device__ __forceinline__ bool column_segment(const SplitParams &p, const DevGroup &G, const DevGCol &C,
                                                int64_t c, int r0, double (&v)[16]) {
+  if (C.start >= G.nrows || r0 >= G.nrows || r0 + 16 <= C.start) return false;
+  if (C.kind == 1 && r0 >= C.start && r0 + 16 <= G.nrows) {
+    // steady state: seeds at r0, r0 + 1, recurrence for the other 14 rows
+    const double *seed = p.seeds + G.seeds + (c * G.nchunks + r0 / kSeedRows) * 2;
+    double pp = seed[0], pc = seed[1];
+    const double x2 = p.f64[C.data];
+    const double *ab = p.f64 + C.aux + 3 * (int64_t)(r0 - C.boff);
+    v[0] = pp;
+    v[1] = pc;
+#pragma unroll
+    for (int i = 2; i < 16; ++i) {
+      const double *a = ab + 3 * (i - 2);
+      const double nv = (x2 + a[0]) * a[1] * pc + a[2] * pp;
+      pp = pc;
+      pc = nv;
+      v[i] = nv;
+    }
+    return true;
+  }
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = 0.0;
-  if (C.start >= G.nrows || r0 >= G.nrows || r0 + 16 <= C.start) return;
   if (C.kind == 0) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int r = r0 + i;
       if (r >= C.start && r < G.nrows) v[i] = p.f64[C.data + (r - C.start)];
     }
-    return;
+    return true;
   }
   const int s0 = max(r0, C.start);
   const double *seed = p.seeds + G.seeds + (c * G.nchunks + r0 / kSeedRows) * 2;
@@ -413,10 +432,16 @@ __device__ __forceinline__ void column_segment(const SplitParams &p, const DevGr
       v[i] = nv;
     }
   }
+  return true;
 }
 
 // Scaled digits of 16 values, packed as four words per slice (row i in byte
 // i % 4 of word i / 4), stored as one 16-byte row per slice.
+__device__ __forceinline__ void store_zero_slices(unsigned char *dst) {
+#pragma unroll
+  for (int sl = 0; sl < kSplitSlices; ++sl) *reinterpret_cast<uint4 *>(dst + sl * kSliceA) = make_uint4(0, 0, 0, 0);
+}
+
 __device__ __forceinline__ void store_slices(unsigned char *dst, const double (&v)[16], const double *scale,
                                              int scale_stride) {
   uint32_t w[kSplitSlices][4];
@@ -439,15 +464,15 @@ struct Pipe {
   int stage;
 };
 
-// Waits for the MMAs that last read the current stage; false (CTA-uniform)
-// on expiry.
+// Waits (this thread) for the MMAs that last read the current stage; false on
+// expiry.  The CTA agrees on the outcome at the next stage_issue.
 __device__ __forceinline__ bool stage_free(SplitSmem *ss, Pipe &q) {
   const int s = q.stage;
   if (!q.pending[s]) return true;
   const bool ok = mbar_wait(&ss->bar[s], q.phase[s]);
   q.phase[s] ^= 1u;
   q.pending[s] = false;
-  return !__syncthreads_or(!ok);
+  return ok;
 }
 
 // Waits for every outstanding MMA; false (CTA-uniform) on expiry.
@@ -462,22 +487,28 @@ __device__ __forceinline__ bool pipe_drain(SplitSmem *ss, Pipe &q) {
   return !__syncthreads_or(!ok);
 }
 
-// Copies the operand-B chunk into the stage, then (one thread) issues the
-// two K steps of MMAs on it and commits them to the stage's mbarrier.
-__device__ __forceinline__ void stage_issue(const SplitParams &p, unsigned char *smem, SplitSmem *ss, Pipe &q,
-                                            uint32_t tmem, int64_t plane, int a_mn, bool first) {
-  unsigned char *A = smem + q.stage * kStageA;
-  unsigned char *B = smem + 2 * kStageA + q.stage * kStageB;
-  {
-    const uint4 *src = reinterpret_cast<const uint4 *>(p.planes + plane * (int64_t)kSplitPlane);
-    uint4 *dst = reinterpret_cast<uint4 *>(B);
-    for (int i = threadIdx.x; i < kStageB / 16; i += kSplitThr) dst[i] = src[i];
-  }
+// Starts the asynchronous copy of an operand-B chunk into the current stage.
+__device__ __forceinline__ void stage_load_b(const SplitParams &p, unsigned char *smem, const Pipe &q, int64_t plane) {
+  const unsigned char *src = reinterpret_cast<const unsigned char *>(p.planes) + plane * (int64_t)kSplitPlane;
+  const uint32_t dst = smem_u32(smem + 2 * kStageA + q.stage * kStageB);
+  for (int i = threadIdx.x; i < kStageB / 16; i += kSplitThr)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16 * i), "l"(src + 16 * i) : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Completes the stage (B copy, A stores of all threads), agrees on `ok`
+// across the CTA, then (one thread) issues the two K steps of MMAs on it and
+// commits them to the stage's mbarrier.  Returns false (CTA-uniform) if any
+// thread's wait expired; no MMA is issued then.
+__device__ __forceinline__ bool stage_issue(unsigned char *smem, SplitSmem *ss, Pipe &q, uint32_t tmem, int a_mn,
+                                            bool first, bool ok) {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   fence_operands();
-  __syncthreads();
+  if (__syncthreads_or(!ok)) return false;
   fence_after_sync();
   if (threadIdx.x == 0) {
-    const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
+    const uint32_t a0 = smem_u32(smem + q.stage * kStageA);
+    const uint32_t b0 = smem_u32(smem + 2 * kStageA + q.stage * kStageB);
     for (int ks = 0; ks < kSplitK / 32; ++ks) {
       if (a_mn) issue_step(tmem, a0 + ks * 512, b0 + ks * 256, 1, 128, 1024, first && ks == 0);
       else issue_step(tmem, a0 + ks * 256, b0 + ks * 256, 0, 128, 512, first && ks == 0);
@@ -486,6 +517,7 @@ __device__ __forceinline__ void stage_issue(const SplitParams &p, unsigned char 
   }
   q.pending[q.stage] = true;
   q.stage ^= 1;
+  return true;
 }
 
 // Epilogue: lane = M row of the unit; warps w, w + 4, w + 8, w + 12 share a
@@ -561,14 +593,16 @@ __global__ void __launch_bounds__(kSplitThr, 1) k_a2m_split(SplitParams p) {
       C.start = G.nrows;
     }
     for (int kc = T.kc0; kc < S.nrchunks; ++kc) {
-      if (!stage_free(ss, q)) {
+      const bool ok = stage_free(ss, q);
+      stage_load_b(p, smem, q, S.apl + kc);
+      double v[16];
+      unsigned char *dst = smem + q.stage * kStageA + (c >> 3) * 512 + seg * 128 + (c & 7) * 16;
+      if (column_segment(p, G, C, gc, kc * kSplitK + 16 * seg, v)) store_slices(dst, v, &csc.x, 0);
+      else store_zero_slices(dst);
+      if (!stage_issue(smem, ss, q, tmem, 0, kc == T.kc0, ok)) {
         abort = true;
         break;
       }
-      double v[16];
-      column_segment(p, G, C, gc, kc * kSplitK + 16 * seg, v);
-      store_slices(smem + q.stage * kStageA + (c >> 3) * 512 + seg * 128 + (c & 7) * 16, v, &csc.x, 0);
-      stage_issue(p, smem, ss, q, tmem, S.apl + kc, 0, kc == T.kc0);
     }
     if (abort || !pipe_drain(ss, q)) {
       abort = true;
@@ -623,19 +657,20 @@ __global__ void __launch_bounds__(kSplitThr, 1) k_m2a_split(SplitParams p) {
     __syncthreads();
     const int r0 = T.row0 + 16 * seg;
     for (int kc = 0; kc < S.ncchunks; ++kc) {
-      if (!stage_free(ss, q)) {
-        abort = true;
-        break;
-      }
+      const bool ok = stage_free(ss, q);
+      stage_load_b(p, smem, q, S.xpl + kc);
       const int64_t gc = (int64_t)kc * kSplitK + cl;
       DevGCol C{};
       if (gc < G.ncols) C = p.gcols[G.cols + gc];
       else C.start = G.nrows;
       double v[16];
-      column_segment(p, G, C, gc, r0, v);
-      store_slices(smem + q.stage * kStageA + seg * 1024 + (cl >> 3) * 128 + (cl & 7) * 16, v,
-                   &rsc[16 * seg].x, 2);
-      stage_issue(p, smem, ss, q, tmem, S.xpl + kc, 1, kc == 0);
+      unsigned char *dst = smem + q.stage * kStageA + seg * 1024 + (cl >> 3) * 128 + (cl & 7) * 16;
+      if (column_segment(p, G, C, gc, r0, v)) store_slices(dst, v, &rsc[16 * seg].x, 2);
+      else store_zero_slices(dst);
+      if (!stage_issue(smem, ss, q, tmem, 1, kc == 0, ok)) {
+        abort = true;
+        break;
+      }
     }
     if (abort || !pipe_drain(ss, q)) {
       abort = true;

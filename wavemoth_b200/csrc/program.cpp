@@ -577,6 +577,10 @@ bool build_fast_path(HostProgram &P, std::string &err) {
         }
       }
       G.ncols = (int32_t)(P.gcols.size() - G.cols);
+      // columns by first active row, so that the column tiles of the
+      // tensor-core kernels span similar row ranges
+      std::stable_sort(P.gcols.begin() + G.cols, P.gcols.end(),
+                       [](const DevGCol &a, const DevGCol &b) { return a.start < b.start; });
       G.nchunks = (G.nrows + kSeedRows - 1) / kSeedRows;
       G.seeds = P.nseeds;
       P.nseeds += 2LL * G.ncols * G.nchunks;

@@ -100,7 +100,7 @@ class Transform:
     def work(self):
         """Algorithmic work of one direction (see wavemoth_plan_work)."""
         import ctypes
-        out = (ctypes.c_double * 8)()
+        out = (ctypes.c_double * 12)()
         rc = _native.lib().wavemoth_plan_work(self._plan, self.nmaps, out)
         if rc != 0:
             raise WavemothError("work query failed: " + last_error())
@@ -108,6 +108,8 @@ class Transform:
         return {"legendre_flops": o[0], "matrix_bytes": o[1], "legendre_vector_bytes": o[2],
                 "ring_bytes": o[3], "interp_elems": o[4], "rec_elems": o[5], "dense_elems": o[6],
                 "legendre_grid": o[7],
+                "split_elems_alm2map": o[8], "split_elems_map2alm": o[9],
+                "split_int8_ops_alm2map": o[10], "split_int8_ops_map2alm": o[11],
                 "device_bytes": _native.lib().wavemoth_plan_device_bytes(self._plan),
                 "program_bytes": _native.lib().wavemoth_plan_program_bytes(self._plan)}
 
