@@ -163,6 +163,7 @@ struct RingTable {
   int32_t ntasks0 = 0, ntasks1 = 0;
   int32_t smem0 = 0, smem1 = 0;
   int32_t nphase_hi = 1;
+  int64_t max_cta_cplx = 0;  // largest transform buffer of one CTA
 };
 
 // Ring geometry (src/wavemoth.c:1199-1232) and the CTA work list of the ring
@@ -230,6 +231,7 @@ RingTable ring_table(int nside, int nmaps, int mmax) {
     int lg = 0;
     while ((1 << lg) < G) ++lg;
     const double cost = (double)G * len * (R.bluestein_m ? 2.5 : 1.0) + (double)G * (mmax + 1);
+    T.max_cta_cplx = std::max(T.max_cta_cplx, (int64_t)G * len);
     for (int g0 = 0; g0 < nmaps; g0 += G)
       items.push_back({cost, wm::DevRingTask{r, g0, lg, 0}, cls, (int64_t)G * len});
   }
@@ -398,6 +400,8 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   rc = rc ? rc : A.alloc(&P->d_xbuf, (size_t)std::max<int64_t>(G.xrows, 1) * P->nvecs, "X buffer");
   {
     RingTable RT = ring_table(P->nside, nmaps, mmax);
+    if (!rc && RT.max_cta_cplx > 2 * wm::kRingBufferCplx)
+      rc = set_error(WAVEMOTH_ERR_ARG, "ring transforms longer than 8192 points (nside > 2048) are not supported");
     P->twlen = RT.twlen;
     P->max_bluestein = RT.max_bluestein;
     P->ring_ntasks0 = RT.ntasks0;

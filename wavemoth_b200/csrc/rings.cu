@@ -14,34 +14,40 @@
 //   ring[2s] = Re z[s], ring[2s+1] = Im z[s],  z = IDFT_N(Z)
 // and the analysis r2c uses the mirror identity.
 //
-// Length-N transforms, in place in shared memory:
-//   * N a power of two (every belt ring): radix-2^2 Cooley-Tukey passes.  The
-//     inverse reads its input in bit-reversed order (Z is stored there as it
-//     is formed) and writes natural order; the forward (decimation in
-//     frequency) reads natural order and leaves the spectrum bit-reversed.
+// Length-N transforms, in place in shared memory, as passes of radix 16 (and
+// one pass of radix 2, 4 or 8 when log2 of the length is not a multiple of
+// 4); a pass loads 16 points per butterfly into registers and runs four
+// radix-2 stages there:
+//   * N a power of two (every belt ring): synthesis by decimation in
+//     frequency (natural order in, bit-reversed out), analysis by decimation
+//     in time (bit-reversed in, natural out).  Z is formed in natural order
+//     as W is gathered from q, the last synthesis pass writes the ring
+//     pixels from its registers and the first analysis pass loads them.
 //   * any other N (polar rings, n = 4i): Bluestein's chirp-z identity
 //     jk = (j^2 + k^2 - (k - j)^2) / 2 turns the DFT into a cyclic convolution
-//     of length M = 2^p >= 2N - 1: forward decimation-in-frequency FFT of the
-//     chirped input (bit-reversed spectrum), product with the chirp filter's
-//     spectrum (precomputed per ring at plan creation, stored bit-reversed),
-//     inverse decimation-in-time FFT back to natural order.
-// Twiddles come from one table of e^{2 pi i k / TW}, TW the largest power of
-// two used; the chirps e^{i pi k^2 / N} and roots e^{2 pi i k / n} of the
-// Bluestein rings from a per-ring table; all are computed once, at plan
-// creation, with sincospi on exact rationals.
+//     of length M = 2^p >= 2N - 1: DIF of the chirped, zero-padded input, the
+//     product with the chirp filter's spectrum (precomputed per ring, stored
+//     in the DIF output order) and DIT back; the last DIF pass, the product
+//     and the first DIT pass share one register pass.
+// Within a radix-16 pass the twiddles of radix-2 stage s at offset
+// j + m (len / 16) factor as w_{len / 2^s}^j (one table lookup per stage)
+// times a 16th root of unity fixed at compile time.  Twiddles come from one
+// table of e^{2 pi i k / TW}, TW the largest power of two used; chirps
+// e^{i pi k^2 / N} and roots e^{2 pi i k / n} of the Bluestein rings from a
+// per-ring table; all computed at plan creation with sincospi on exact
+// rationals.
 //
 // Work decomposition: one CTA per (ring pair, group of G = 2^lg maps), G
 // chosen per ring so that the transform buffer (G x N or G x M complex) fits
-// 64 KB and three CTAs share an SM.  The G maps are the fastest index of the
-// CTA's thread layout: lanes g = 0..G-1 of a warp handle the same bin, pixel
-// or butterfly of G maps, so
-//   * q rows (16 bytes per map, maps adjacent) are read as G x 16-byte runs,
-//   * map pixels (8 bytes per map, maps adjacent) are written as G x 8-byte runs,
-//   * twiddles, chirps and phase factors are shared by the G lanes.
+// 64 KB (4096 complex: 16 points per thread at 256 threads); longer
+// transforms run one map per CTA of 512 threads.  The G maps are the fastest
+// index of the thread layout: lanes g = 0..G-1 of a warp handle the same
+// bin, pixel or butterfly of G maps, so q rows and map pixels are read and
+// written as G-map runs and twiddles, chirps and phases are shared.
 // In shared memory element i of map lane g is at slot(i) * G + g with the XOR
-// swizzle slot(i) = i ^ ((i >> 3) & 7), a permutation inside each aligned
-// group of 8 that spreads the 16-byte accesses of every radix-4 and radix-2
-// pass over the 32 banks.
+// swizzle slot(i) = i ^ ((i >> 4) & 15), a permutation inside each aligned
+// group of 16 that makes the 16-byte accesses of every pass of radix 2..16
+// conflict-free for G = 1, 2, 4, 8.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -52,8 +58,9 @@ namespace wm {
 
 namespace {
 
-constexpr int kRingThreads = 256;
-constexpr int kPhaseLo = 64;  // e^{i m phi0} = hi[m / 64] * lo[m % 64]
+constexpr int kRingThreads = 256;      // class 0: <= 4096 complex per CTA
+constexpr int kRingThreadsWide = 512;  // class 1: <= 8192 complex per CTA
+constexpr int kPhaseLo = 64;           // e^{i m phi0} = hi[m / 64] * lo[m % 64]
 
 struct cplx {
   double x, y;
@@ -78,92 +85,201 @@ __device__ __forceinline__ unsigned bitrev(unsigned k, int bits) {
 
 __device__ __forceinline__ int ilog2(int v) { return 31 - __clz(v); }
 
-__device__ __forceinline__ int slot(int i) { return i ^ ((i >> 3) & 7); }
+__device__ __forceinline__ int slot(int i) { return i ^ ((i >> 4) & 15); }
 __device__ __forceinline__ int at(int i, int g, int lg) { return (slot(i) << lg) + g; }
 
-// tw[k] = e^{2 pi i k / twlen}; returns its conjugate for sign -1
-__device__ __forceinline__ cplx twiddle(const double2 *tw, int k, int sign) {
+// tw[k] = e^{2 pi i k / twlen}; its conjugate for SIGN = -1
+template <int SIGN>
+__device__ __forceinline__ cplx twiddle(const double2 *tw, int k) {
   const double2 t = tw[k];
-  return {t.x, sign * t.y};
+  return {t.x, SIGN * t.y};
 }
 
-// In-place DIF over the 2^lg interleaved sequences of length M (a power of
-// two), natural order in, bit-reversed out.  Consecutive radix-2 stages
-// (len, len/2) are fused into one pass (radix 2^2).
-__device__ void fft_dif(cplx *x, int M, int lg, const double2 *tw, int twlen, int sign) {
-  const int gm = (1 << lg) - 1;
-  const int total = (M >> 2) << lg;
+// a e^{SIGN 2 pi i k / 16} for a k known after unrolling
+template <int SIGN>
+__device__ __forceinline__ cplx mul_root16(cplx a, int k) {
+  // cos and sin of 2 pi k / 16, k = 0..3 (the rest by symmetry)
+  constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+  constexpr double h = 0.70710678118654752440;
+  k &= 15;
+  if (k == 0) return a;
+  if (k == 4) return SIGN > 0 ? cplx{-a.y, a.x} : cplx{a.y, -a.x};
+  if (k == 8) return {-a.x, -a.y};
+  if (k == 12) return SIGN > 0 ? cplx{a.y, -a.x} : cplx{-a.y, a.x};
+  double c, s;
+  switch (k & 3) {
+    case 1: c = c1; s = s1; break;
+    case 2: c = h; s = h; break;
+    default: c = s1; s = c1; break;
+  }
+  // quadrant of k: rotate (c, s) by multiples of pi/2
+  const int qd = k >> 2;
+  double cc = c, ss = s;
+  if (qd == 1) { cc = -s; ss = c; }
+  else if (qd == 2) { cc = -c; ss = -s; }
+  else if (qd == 3) { cc = s; ss = -c; }
+  return cmul(a, cplx{cc, SIGN * ss});
+}
+
+template <int R>
+struct Log2;
+template <> struct Log2<2> { static constexpr int v = 1; };
+template <> struct Log2<4> { static constexpr int v = 2; };
+template <> struct Log2<8> { static constexpr int v = 3; };
+template <> struct Log2<16> { static constexpr int v = 4; };
+
+// Radix-R decimation-in-frequency butterfly of the points j + i (len / R),
+// i < R, of one block of length len: log2 R radix-2 stages in registers.
+template <int R, int SIGN>
+__device__ __forceinline__ void dif_regs(cplx (&x)[R], int j, int len, const double2 *tw, int twlen) {
+#pragma unroll
+  for (int s = 0; s < Log2<R>::v; ++s) {
+    const int h = R >> (s + 1);
+    const cplx A = twiddle<SIGN>(tw, j * (twlen / (len >> s)));  // w_{len / 2^s}^j
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) {
+      const int lo = (i / h) * 2 * h + (i % h), hi = lo + h, m = i % h;
+      const cplx u = x[lo], v = x[hi];
+      x[lo] = cadd(u, v);
+      x[hi] = mul_root16<SIGN>(cmul(csub(u, v), A), (m << s) * (16 / R));
+    }
+  }
+}
+
+// Radix-R decimation-in-time butterfly of the points j + i (len / R).
+template <int R, int SIGN>
+__device__ __forceinline__ void dit_regs(cplx (&x)[R], int j, int len, const double2 *tw, int twlen) {
+#pragma unroll
+  for (int s = 0; s < Log2<R>::v; ++s) {
+    const int h = 1 << s;
+    const cplx A = twiddle<SIGN>(tw, j * (twlen / ((len / R) << (s + 1))));  // w_L^j
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) {
+      const int lo = (i / h) * 2 * h + (i % h), hi = lo + h, m = i % h;
+      const cplx u = x[lo];
+      const cplx t = mul_root16<SIGN>(cmul(x[hi], A), m << (4 - (s + 1)));
+      x[lo] = cadd(u, t);
+      x[hi] = csub(u, t);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace wm
+
+namespace wm {
+namespace {
+
+// One in-place pass of radix R over the 2^lg interleaved sequences of length
+// M: butterfly b of lane g takes the points base + i q (q = len / R) of its
+// block, through `load(index, g)` and `store(index, g, value)`.
+template <int R, int SIGN, bool DIF, class LoadF, class StoreF>
+__device__ __forceinline__ void fft_pass(int M, int len, int lg, const double2 *tw, int twlen, LoadF load,
+                                         StoreF store) {
+  const int gm = (1 << lg) - 1, q = len / R, lq = ilog2(q);
+  const int nbf = (M / R) << lg;
+  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
+    const int g = t & gm, b = t >> lg;
+    const int j = b & (q - 1), base = (b >> lq) * len + j;
+    cplx x[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) x[i] = load(base + i * q, g);
+    if (DIF) dif_regs<R, SIGN>(x, j, len, tw, twlen);
+    else dit_regs<R, SIGN>(x, j, len, tw, twlen);
+#pragma unroll
+    for (int i = 0; i < R; ++i) store(base + i * q, g, x[i]);
+  }
+  __syncthreads();
+}
+
+template <int SIGN, bool DIF, class LoadF, class StoreF>
+__device__ __forceinline__ void fft_pass_r(int R, int M, int len, int lg, const double2 *tw, int twlen,
+                                           LoadF load, StoreF store) {
+  switch (R) {
+    case 2: fft_pass<2, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    case 4: fft_pass<4, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    case 8: fft_pass<8, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    default: fft_pass<16, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+  }
+}
+
+// Middle of Bluestein's convolution on blocks of R points (R = the last DIF
+// radix = the first DIT radix): forward DIF stages, the product with the
+// filter spectrum (stored in DIF output order; the sign -1 filter is its
+// reflection F'(k) = conj F(-k)), inverse DIT stages.
+template <int R, class LoadF, class StoreF>
+__device__ __forceinline__ void bluestein_mid_r(int M, int lg, const cplx *F, int fsign, const double2 *tw,
+                                                int twlen, LoadF load, StoreF store) {
+  const int gm = (1 << lg) - 1, bitsM = ilog2(M);
+  const int nbf = (M / R) << lg;
+  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
+    const int g = t & gm, base = (t >> lg) * R;
+    cplx x[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) x[i] = load(base + i, g);
+    dif_regs<R, -1>(x, 0, R, tw, twlen);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int k = base + i;
+      cplx f;
+      if (fsign > 0) {
+        f = F[k];
+      } else {
+        const unsigned natural = bitrev((unsigned)k, bitsM);
+        const unsigned refl = (M - natural) & (M - 1);
+        f = cconj(F[bitrev(refl, bitsM)]);
+      }
+      x[i] = cmul(x[i], f);
+    }
+    dit_regs<R, 1>(x, 0, R, tw, twlen);
+#pragma unroll
+    for (int i = 0; i < R; ++i) store(base + i, g, x[i]);
+  }
+  __syncthreads();
+}
+
+template <class LoadF, class StoreF>
+__device__ __forceinline__ void bluestein_mid(int R, int M, int lg, const cplx *F, int fsign, const double2 *tw,
+                                              int twlen, LoadF load, StoreF store) {
+  switch (R) {
+    case 2: bluestein_mid_r<2>(M, lg, F, fsign, tw, twlen, load, store); break;
+    case 4: bluestein_mid_r<4>(M, lg, F, fsign, tw, twlen, load, store); break;
+    case 8: bluestein_mid_r<8>(M, lg, F, fsign, tw, twlen, load, store); break;
+    default: bluestein_mid_r<16>(M, lg, F, fsign, tw, twlen, load, store); break;
+  }
+}
+
+// Pass radices of a length-M transform in DIF order: 2^(log2 M mod 4) (if
+// above 1) then 16s.  DIT runs them in reverse order.
+struct Radices {
+  int n;         // number of passes
+  int r[5];      // radix of DIF pass p
+  int len[5];    // block length of DIF pass p (the DIT pass mirroring it has the same)
+};
+
+__device__ __forceinline__ Radices radices(int M) {
+  Radices s;
+  const int lgM = ilog2(M), r0 = lgM & 3;
+  s.n = 0;
   int len = M;
-  for (; len >= 4; len >>= 2) {
-    const int q = len >> 2, lq = ilog2(q), step = twlen / len;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int g = t & gm, b = t >> lg;
-      const int j = b & (q - 1), base = ((b >> lq) << (lq + 2)) + j;
-      const int i0 = at(base, g, lg), i1 = at(base + q, g, lg);
-      const int i2 = at(base + 2 * q, g, lg), i3 = at(base + 3 * q, g, lg);
-      const cplx a0 = x[i0], a1 = x[i1], a2 = x[i2], a3 = x[i3];
-      const cplx w1 = twiddle(tw, j * step, sign), w1b = twiddle(tw, (j + q) * step, sign);
-      const cplx w2 = twiddle(tw, 2 * j * step, sign);
-      const cplx b0 = cadd(a0, a2), b2 = cmul(csub(a0, a2), w1);
-      const cplx b1 = cadd(a1, a3), b3 = cmul(csub(a1, a3), w1b);
-      x[i0] = cadd(b0, b1);
-      x[i1] = cmul(csub(b0, b1), w2);
-      x[i2] = cadd(b2, b3);
-      x[i3] = cmul(csub(b2, b3), w2);
-    }
-    __syncthreads();
+  if (r0) {
+    s.r[s.n] = 1 << r0;
+    s.len[s.n++] = len;
+    len >>= r0;
   }
-  if (len == 2) {
-    for (int t = threadIdx.x; t < ((M >> 1) << lg); t += blockDim.x) {
-      const int g = t & gm, b = t >> lg;
-      const int i0 = at(2 * b, g, lg), i1 = at(2 * b + 1, g, lg);
-      const cplx u = x[i0], v = x[i1];
-      x[i0] = cadd(u, v);
-      x[i1] = csub(u, v);
-    }
-    __syncthreads();
+  for (int k = 0; k < (lgM >> 2); ++k) {
+    s.r[s.n] = 16;
+    s.len[s.n++] = len;
+    len >>= 4;
   }
+  return s;
 }
 
-// In-place DIT over 2^lg interleaved sequences: bit-reversed in, natural out;
-// stages (L, 2L) fused.
-__device__ void fft_dit(cplx *x, int M, int lg, const double2 *tw, int twlen, int sign) {
-  const int gm = (1 << lg) - 1;
-  const int total = (M >> 2) << lg;
-  int L = 2;
-  if (ilog2(M) & 1) {
-    for (int t = threadIdx.x; t < ((M >> 1) << lg); t += blockDim.x) {
-      const int g = t & gm, b = t >> lg;
-      const int i0 = at(2 * b, g, lg), i1 = at(2 * b + 1, g, lg);
-      const cplx u = x[i0], v = x[i1];
-      x[i0] = cadd(u, v);
-      x[i1] = csub(u, v);
-    }
-    __syncthreads();
-    L = 4;
-  }
-  for (; L <= M / 2; L <<= 2) {
-    const int q = L >> 1, lq = ilog2(q), len = 2 * L;
-    const int s1 = twlen / L, s2 = twlen / len;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int g = t & gm, b = t >> lg;
-      const int j = b & (q - 1), base = ((b >> lq) << (lq + 2)) + j;
-      const int i0 = at(base, g, lg), i1 = at(base + q, g, lg);
-      const int i2 = at(base + 2 * q, g, lg), i3 = at(base + 3 * q, g, lg);
-      const cplx a0 = x[i0], a1 = x[i1], a2 = x[i2], a3 = x[i3];
-      const cplx w1 = twiddle(tw, j * s1, sign);
-      const cplx w2 = twiddle(tw, j * s2, sign), w2b = twiddle(tw, (j + q) * s2, sign);
-      const cplx t1 = cmul(a1, w1), t3 = cmul(a3, w1);
-      const cplx b0 = cadd(a0, t1), b1 = csub(a0, t1), b2 = cadd(a2, t3), b3 = csub(a2, t3);
-      const cplx u2 = cmul(b2, w2), u3 = cmul(b3, w2b);
-      x[i0] = cadd(b0, u2);
-      x[i2] = csub(b0, u2);
-      x[i1] = cadd(b1, u3);
-      x[i3] = csub(b1, u3);
-    }
-    __syncthreads();
-  }
-}
+}  // namespace
+}  // namespace wm
+
+namespace wm {
+namespace {
 
 // e^{i pi num / den} for an exact rational, reduced modulo 2 first
 __device__ __forceinline__ cplx expi_pi(long long num, long long den) {
@@ -210,7 +326,7 @@ __device__ __forceinline__ cplx phase_at(const cplx *lo, const cplx *hi, int m) 
 struct RingCta {
   DevRing R;
   int ring, map0, lg, nm;  // nm: maps of the group that exist
-  int n, N, M, bits, bitsM;
+  int n, N, M, bits;
   bool pow2;
 };
 
@@ -227,39 +343,12 @@ __device__ __forceinline__ RingCta ring_cta(const RingParams &p, int task) {
   c.pow2 = c.R.bluestein_m == 0;
   c.M = c.pow2 ? c.N : c.R.bluestein_m;
   c.bits = ilog2(c.N);
-  c.bitsM = ilog2(c.M);
   return c;
 }
 
-// Cyclic convolution step of Bluestein's method on the chirped, zero-padded
-// buffer (natural order in, natural order out).
-__device__ void bluestein_convolve(cplx *buf, const RingCta &c, const RingParams &p, int sign) {
-  const int gm = (1 << c.lg) - 1, M = c.M;
-  fft_dif(buf, M, c.lg, p.twiddles, p.twlen, -1);
-  // filter spectrum, stored bit-reversed for sign +1; the sign -1 filter is
-  // its reflection F'(k) = F(-k), conjugated
-  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
-  for (int t = threadIdx.x; t < (M << c.lg); t += blockDim.x) {
-    const int g = t & gm, k = t >> c.lg;
-    cplx f;
-    if (sign > 0) {
-      f = F[k];
-    } else {
-      const unsigned natural = bitrev((unsigned)k, c.bitsM);
-      const unsigned refl = (M - natural) & (M - 1);
-      f = cconj(F[bitrev(refl, c.bitsM)]);
-    }
-    const int i = at(k, g, c.lg);
-    buf[i] = cmul(buf[i], f);
-  }
-  __syncthreads();
-  fft_dit(buf, M, c.lg, p.twiddles, p.twlen, +1);
-}
-
 // W[j] of one map (q row pointer `qg` at ring r, map g), aliasing sum in increasing m
-__device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mmax,
-                                          int64_t qstride, int64_t half, double sgn,
-                                          const cplx *plo, const cplx *phi) {
+__device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mmax, int64_t qstride,
+                                          int64_t half, double sgn, const cplx *plo, const cplx *phi) {
   cplx acc = {0.0, 0.0};
   for (int base = 0;; base += n) {
     const int m1 = base + j;
@@ -279,21 +368,27 @@ __device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mm
   return acc;
 }
 
-__global__ void __launch_bounds__(kRingThreads, 3) k_ring_synthesis(RingParams p, int task0) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? 2 : 1)
+    k_ring_synthesis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, task0 + blockIdx.x);
-  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N;
+  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N, M = c.M;
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
-  cplx *plo = buf + ((int64_t)c.M << lg);
+  cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
   phase_tables(plo, phi, p, c.R);
   __syncthreads();
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   const double *qbase = p.q + (int64_t)c.ring * p.nvecs + 2 * c.map0;
+  const Radices rs = radices(M);
+  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
+  const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   for (int side = 0; side < 2; ++side) {
     if (side == 1 && c.ring == 0) break;  // the equator is written once
     const double sgn = side ? -1.0 : 1.0;
-    // Z[k] and Z[N - k] from W[k] and W[N - k]
+    // Z[k] and Z[N - k] (natural order, chirped for Bluestein rings) from
+    // W[k] and W[N - k]
     const int npairs = (N >> 1) + 1;
     for (int t = threadIdx.x; t < (npairs << lg); t += blockDim.x) {
       const int g = t & gm, kk = t >> lg, kr = N - kk;
@@ -312,64 +407,111 @@ __global__ void __launch_bounds__(kRingThreads, 3) k_ring_synthesis(RingParams p
           Wk.y = 0.0;
           Wc.y = 0.0;
         }
-        const cplx s = cadd(Wk, Wc), d = csub(Wk, Wc);
-        cplx Z = cadd(s, mul_i(cmul(ring_root(p, c.R, k), d)));
-        if (c.pow2) {
-          buf[at((int)bitrev((unsigned)k, c.bits), g, lg)] = Z;
-        } else {
-          buf[at(k, g, lg)] = cmul(Z, ring_chirp(p, c.R, k));
-        }
+        const cplx sm = cadd(Wk, Wc), d = csub(Wk, Wc);
+        const cplx Z = cadd(sm, mul_i(cmul(ring_root(p, c.R, k), d)));
+        buf[at(k, g, lg)] = c.pow2 ? Z : cmul(Z, ring_chirp(p, c.R, k));
       }
     }
     if (!c.pow2)
-      for (int t = threadIdx.x; t < ((c.M - N) << lg); t += blockDim.x)
+      for (int t = threadIdx.x; t < ((M - N) << lg); t += blockDim.x)
         buf[at(N + (t >> lg), t & gm, lg)] = {0.0, 0.0};
     __syncthreads();
-    if (c.pow2) fft_dit(buf, N, lg, p.twiddles, p.twlen, +1);
-    else bluestein_convolve(buf, c, p, +1);
-    const int64_t off = side ? c.R.off_south : c.R.off_north;
-    const double inv = c.pow2 ? 1.0 : 1.0 / (double)c.M;
-    double *out = p.map + off * p.nmaps + c.map0;
-    for (int t = threadIdx.x; t < (n << lg); t += blockDim.x) {
-      const int g = t & gm, pix = t >> lg, s = pix >> 1;
-      if (g >= c.nm) continue;
-      cplx z = buf[at(s, g, lg)];
-      if (!c.pow2) z = cscale(cmul(z, ring_chirp(p, c.R, s)), inv);
-      out[(int64_t)pix * p.nmaps + g] = (pix & 1) ? z.y : z.x;
+    double *out = p.map + (side ? c.R.off_south : c.R.off_north) * p.nmaps + c.map0;
+    auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, lg)]; };
+    auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, lg)] = v; };
+    // pixels 2s, 2s + 1 of output z[s]; power of two: DIF position pos holds z[bitrev(pos)]
+    auto pix_dif = [&](int pos, int g, cplx z) {
+      if (g >= c.nm) return;
+      const int64_t s = bitrev((unsigned)pos, c.bits);
+      out[(2 * s) * p.nmaps + g] = z.x;
+      out[(2 * s + 1) * p.nmaps + g] = z.y;
+    };
+    auto pix_blue = [&](int k, int g, cplx z) {
+      if (k >= N || g >= c.nm) return;
+      z = cscale(cmul(z, ring_chirp(p, c.R, k)), inv);
+      out[(2 * (int64_t)k) * p.nmaps + g] = z.x;
+      out[(2 * (int64_t)k + 1) * p.nmaps + g] = z.y;
+    };
+    if (c.pow2) {
+      for (int ps = 0; ps < rs.n; ++ps) {
+        if (ps == rs.n - 1) fft_pass_r<1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, pix_dif);
+        else fft_pass_r<1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+      }
+    } else {
+      for (int ps = 0; ps < rs.n - 1; ++ps)
+        fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+      const int R = rs.r[rs.n - 1];
+      if (rs.n == 1) {
+        bluestein_mid(R, M, lg, F, +1, p.twiddles, p.twlen, sload, pix_blue);
+      } else {
+        bluestein_mid(R, M, lg, F, +1, p.twiddles, p.twlen, sload, sstore);
+        for (int ps = rs.n - 2; ps >= 0; --ps) {
+          if (ps == 0) fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, pix_blue);
+          else fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+        }
+      }
     }
-    __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kRingThreads, 3) k_ring_analysis(RingParams p, int task0) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? 2 : 1)
+    k_ring_analysis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, task0 + blockIdx.x);
-  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N;
+  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N, M = c.M;
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
-  cplx *plo = buf + ((int64_t)c.M << lg);
+  cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
   phase_tables(plo, phi, p, c.R);
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   double *qbase = p.q_out + (int64_t)c.ring * p.nvecs + 2 * c.map0;
-  const double inv = c.pow2 ? 1.0 : 1.0 / (double)c.M;
+  const Radices rs = radices(M);
+  const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
+  const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   for (int side = 0; side < 2; ++side) {
     if (side == 1 && c.ring == 0) break;
-    const int64_t off = side ? c.R.off_south : c.R.off_north;
-    const double *in = p.map_in + off * p.nmaps + c.map0;
-    for (int t = threadIdx.x; t < (N << lg); t += blockDim.x) {
-      const int g = t & gm, s = t >> lg;
-      cplx z = {0.0, 0.0};
-      if (g < c.nm) z = {in[(int64_t)(2 * s) * p.nmaps + g], in[(int64_t)(2 * s + 1) * p.nmaps + g]};
-      if (!c.pow2) z = cmul(z, cconj(ring_chirp(p, c.R, s)));
-      buf[at(s, g, lg)] = z;
+    const double *in = p.map_in + (side ? c.R.off_south : c.R.off_north) * p.nmaps + c.map0;
+    auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, lg)]; };
+    auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, lg)] = v; };
+    // power of two: the DIT input position pos holds z[bitrev(pos)]
+    auto pix_dit = [&](int pos, int g) -> cplx {
+      if (g >= c.nm) return {0.0, 0.0};
+      const int64_t s = bitrev((unsigned)pos, c.bits);
+      return {in[(2 * s) * p.nmaps + g], in[(2 * s + 1) * p.nmaps + g]};
+    };
+    // Bluestein: chirped input z[k], zero beyond N
+    auto pix_blue = [&](int k, int g) -> cplx {
+      if (k >= N || g >= c.nm) return {0.0, 0.0};
+      const cplx z = {in[(2 * (int64_t)k) * p.nmaps + g], in[(2 * (int64_t)k + 1) * p.nmaps + g]};
+      return cmul(z, cconj(ring_chirp(p, c.R, k)));
+    };
+    auto zstore = [&](int k, int g, cplx v) {
+      if (k < N) buf[at(k, g, lg)] = cscale(cmul(v, cconj(ring_chirp(p, c.R, k))), inv);
+    };
+    if (c.pow2) {
+      for (int ps = rs.n - 1; ps >= 0; --ps) {
+        if (ps == rs.n - 1) fft_pass_r<-1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, pix_dit, sstore);
+        else fft_pass_r<-1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+      }
+    } else {
+      for (int ps = 0; ps < rs.n - 1; ++ps) {
+        if (ps == 0) fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, pix_blue, sstore);
+        else fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+      }
+      const int R = rs.r[rs.n - 1];
+      if (rs.n == 1) {
+        bluestein_mid(R, M, lg, F, -1, p.twiddles, p.twlen, pix_blue, zstore);
+      } else {
+        bluestein_mid(R, M, lg, F, -1, p.twiddles, p.twlen, sload, sstore);
+        for (int ps = rs.n - 2; ps >= 0; --ps) {
+          if (ps == 0) fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, zstore);
+          else fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+        }
+      }
     }
-    if (!c.pow2)
-      for (int t = threadIdx.x; t < ((c.M - N) << lg); t += blockDim.x)
-        buf[at(N + (t >> lg), t & gm, lg)] = {0.0, 0.0};
-    __syncthreads();
-    if (c.pow2) fft_dif(buf, N, lg, p.twiddles, p.twlen, -1);
-    else bluestein_convolve(buf, c, p, -1);
-    // fold the spectrum F[k] (k <= N) into q~: g_m = F[m mod n] or its mirror
+    // fold the spectrum F[k] (k <= N, from Z in natural order) into q~:
+    // g_m = F[m mod n] or its mirror
     for (int t = threadIdx.x; t < ((p.mmax + 1) << lg); t += blockDim.x) {
       const int g = t & gm, m = t >> lg;
       if (g >= c.nm) continue;
@@ -377,21 +519,14 @@ __global__ void __launch_bounds__(kRingThreads, 3) k_ring_analysis(RingParams p,
       const bool mirror = jm > N;
       const int k = mirror ? n - jm : jm;
       const int k1 = k == N ? 0 : k, k2 = k == 0 ? 0 : N - k;
-      cplx Zk, Zc;
-      if (c.pow2) {
-        Zk = buf[at((int)bitrev((unsigned)k1, c.bits), g, lg)];
-        Zc = buf[at((int)bitrev((unsigned)k2, c.bits), g, lg)];
-      } else {
-        Zk = cscale(cmul(buf[at(k1, g, lg)], cconj(ring_chirp(p, c.R, k1))), inv);
-        Zc = cscale(cmul(buf[at(k2, g, lg)], cconj(ring_chirp(p, c.R, k2))), inv);
-      }
-      Zc = cconj(Zc);
+      const cplx Zk = buf[at(k1, g, lg)];
+      const cplx Zc = cconj(buf[at(k2, g, lg)]);
       const cplx E = cscale(cadd(Zk, Zc), 0.5);
       const cplx D = csub(Zk, Zc);
       const cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
-      cplx F = cadd(E, cmul(cconj(ring_root(p, c.R, k)), O));
-      if (mirror) F = cconj(F);
-      const cplx gv = cscale(cmul(F, cconj(phase_at(plo, phi, m))), p.scale);
+      cplx Fk = cadd(E, cmul(cconj(ring_root(p, c.R, k)), O));
+      if (mirror) Fk = cconj(Fk);
+      const cplx gv = cscale(cmul(Fk, cconj(phase_at(plo, phi, m))), p.scale);
       double *qe = qbase + m * qstride + 2 * g;
       double *qo = qe + half;
       if (side == 0) {
@@ -430,7 +565,7 @@ __global__ void k_ring_aux(RingParams p) {
   }
 }
 
-__global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p) {
+__global__ void __launch_bounds__(kRingThreadsWide) k_bluestein_filters(RingParams p) {
   extern __shared__ double smem_d[];
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   const DevRing R = p.rings[blockIdx.x];
@@ -444,22 +579,28 @@ __global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p
     buf[at(k, 0, 0)] = v;
   }
   __syncthreads();
-  fft_dif(buf, M, 0, p.twiddles, p.twlen, -1);
+  auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, 0)]; };
+  auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, 0)] = v; };
+  const Radices rs = radices(M);
+  for (int ps = 0; ps < rs.n; ++ps)
+    fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], 0, p.twiddles, p.twlen, sload, sstore);
   cplx *F = reinterpret_cast<cplx *>(p.filters_out) + R.filter;
   for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[at(k, 0, 0)];
 }
 
-template <class K>
-cudaError_t launch_classes(K kernel, const RingParams &prm, cudaStream_t st) {
-  const int smem_max = prm.smem0 > prm.smem1 ? prm.smem0 : prm.smem1;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-  if (e != cudaSuccess) return e;
+template <class K0, class K1>
+cudaError_t launch_classes(K0 kernel0, K1 kernel1, const RingParams &prm, cudaStream_t st) {
+  cudaError_t e;
   if (prm.ntasks0 > 0) {
-    kernel<<<prm.ntasks0, kRingThreads, prm.smem0, st>>>(prm, 0);
+    e = cudaFuncSetAttribute(kernel0, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.smem0);
+    if (e != cudaSuccess) return e;
+    kernel0<<<prm.ntasks0, kRingThreads, prm.smem0, st>>>(prm, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (prm.ntasks1 > 0) {
-    kernel<<<prm.ntasks1, kRingThreads, prm.smem1, st>>>(prm, prm.ntasks0);
+    e = cudaFuncSetAttribute(kernel1, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.smem1);
+    if (e != cudaSuccess) return e;
+    kernel1<<<prm.ntasks1, kRingThreadsWide, prm.smem1, st>>>(prm, prm.ntasks0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -468,15 +609,15 @@ cudaError_t launch_classes(K kernel, const RingParams &prm, cudaStream_t st) {
 }  // namespace
 
 int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi) {
-  return (int32_t)((buffer_cplx + kPhaseLo + nphase_hi) * 2 * sizeof(double));
+  return (int32_t)((buffer_cplx + kPhaseLo + nphase_hi + 8) * 2 * sizeof(double));
 }
 
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
-  return launch_classes(k_ring_synthesis, prm, st);
+  return launch_classes(k_ring_synthesis<kRingThreads>, k_ring_synthesis<kRingThreadsWide>, prm, st);
 }
 
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
-  return launch_classes(k_ring_analysis, prm, st);
+  return launch_classes(k_ring_analysis<kRingThreads>, k_ring_analysis<kRingThreadsWide>, prm, st);
 }
 
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters, double *aux,
@@ -493,7 +634,7 @@ cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *f
   const int smem = prm.max_bluestein_m * 2 * (int)sizeof(double);
   e = cudaFuncSetAttribute(k_bluestein_filters, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_bluestein_filters<<<prm.ni, kRingThreads, smem, st>>>(q);
+  k_bluestein_filters<<<prm.ni, kRingThreadsWide, smem, st>>>(q);
   return cudaGetLastError();
 }
 
