@@ -92,6 +92,10 @@ struct _wavemoth_plan {
   wm::DevSplitTileB *d_stiles_b = nullptr;
   double2 *d_col_scale = nullptr, *d_row_scale = nullptr, *d_vec_scale = nullptr;
   int8_t *d_planes = nullptr;
+  wm::DevSplitRoot *d_sroots = nullptr;
+  wm::DevSplitLevelTile *d_stiles_la = nullptr, *d_stiles_lm = nullptr;
+  int8_t *d_level_a = nullptr;
+  double2 *d_level_rs = nullptr;
   int32_t *d_status = nullptr;
   wm::DevRing *d_rings = nullptr;
   wm::DevRingTask *d_ring_tasks = nullptr;
@@ -303,6 +307,17 @@ wm::SplitParams split_params(wavemoth_plan P) {
   s.ni = P->ni;
   s.xbuf = P->d_xbuf;
   s.status = P->d_status;
+  s.pairs = P->d_pairs;
+  s.i32 = P->d_i32;
+  s.roots = P->d_roots;
+  s.sroots = P->d_sroots;
+  s.tiles_la = P->d_stiles_la;
+  s.tiles_lm = P->d_stiles_lm;
+  s.nroots = (int32_t)G.roots.size();
+  s.ntiles_la = (int32_t)G.stiles_la.size();
+  s.ntiles_lm = (int32_t)G.stiles_lm.size();
+  s.level_a = P->d_level_a;
+  s.level_rs = P->d_level_rs;
   return s;
 }
 
@@ -424,8 +439,16 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
     rc = rc ? rc : upload(A, &P->d_stiles_b, G.stiles_b, "split map2alm tiles");
     rc = rc ? rc : A.alloc(&P->d_col_scale, (size_t)std::max<int64_t>((int64_t)G.gcols.size(), 1), "column scales");
     rc = rc ? rc : A.alloc(&P->d_row_scale, (size_t)std::max<int64_t>(G.split_rows, 1), "row scales");
-    rc = rc ? rc : A.alloc(&P->d_vec_scale, (size_t)std::max<size_t>(G.groups.size(), 1) * wm::kSplitN,
-                           "vector scales");
+    rc = rc ? rc : A.alloc(&P->d_vec_scale, (size_t)std::max<size_t>(G.groups.size() + G.roots.size(), 1) *
+                                                wm::kSplitN, "vector scales");
+    rc = rc ? rc : upload(A, &P->d_sroots, G.sroots, "split roots");
+    rc = rc ? rc : upload(A, &P->d_stiles_la, G.stiles_la, "split alm2map level tiles");
+    rc = rc ? rc : upload(A, &P->d_stiles_lm, G.stiles_lm, "split map2alm level tiles");
+    rc = rc ? rc : A.alloc(&P->d_level_a,
+                           (size_t)std::max<int64_t>(G.split_level_achunks, 1) * wm::kSplitSlices * wm::kSplitM *
+                               wm::kSplitK, "sliced interpolation matrices");
+    rc = rc ? rc : A.alloc(&P->d_level_rs, (size_t)std::max<int64_t>(G.split_level_rows, 1),
+                           "interpolation row scales");
     rc = rc ? rc : A.alloc(&P->d_planes, (size_t)std::max<int64_t>(G.split_chunks, 1) * wm::kSplitPlane,
                            "operand slices");
   }
@@ -464,6 +487,7 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
       sp.colmax = colmax;
       sp.rowmax = rowmax;
       rc = cuda_check(wm::launch_split_scales(sp, P->stream), "split scale launch");
+      if (!rc) rc = cuda_check(wm::launch_level_slices(sp, P->stream), "level slice launch");
       if (!rc) rc = cuda_check(cudaStreamSynchronize(P->stream), "split scales");
     }
     cudaFree(colmax);
@@ -580,12 +604,31 @@ int run_split(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_o
   s.q_in = q_in;
   s.q = q_out;
   const int nt = alm2map ? s.ntiles_a : s.ntiles_b;
+  const int nl = alm2map ? s.ntiles_la : s.ntiles_lm;
+  const int gop = std::min((int)G.groups.size(), 8 * P->sm_count);
+  const int gop_l = std::min(std::max(s.nroots, 1), 8 * P->sm_count);
   for (int v0 = 0; v0 < P->nvecs; v0 += wm::kSplitN) {
     s.v0 = v0;
-    int rc = cuda_check(wm::launch_split(alm2map ? 0 : 2, s, std::min((int)G.groups.size(), 8 * P->sm_count), st),
-                        "operand slice launch");
-    if (!rc && nt)
-      rc = cuda_check(wm::launch_split(alm2map ? 1 : 3, s, std::min(nt, P->sm_count), st), "split GEMM launch");
+    int rc = 0;
+    // alm2map: residual (alm -> X, q) then levels (X -> q); map2alm reversed
+    auto residual = [&]() {
+      rc = cuda_check(wm::launch_split(alm2map ? 0 : 2, s, gop, st), "operand slice launch");
+      if (!rc && nt)
+        rc = cuda_check(wm::launch_split(alm2map ? 1 : 3, s, std::min(nt, P->sm_count), st), "split GEMM launch");
+    };
+    auto levels = [&]() {
+      if (!nl) return;
+      rc = cuda_check(wm::launch_split(alm2map ? 4 : 6, s, gop_l, st), "level operand slice launch");
+      if (!rc)
+        rc = cuda_check(wm::launch_split(alm2map ? 5 : 7, s, std::min(nl, P->sm_count), st), "level GEMM launch");
+    };
+    if (alm2map) {
+      residual();
+      if (!rc) levels();
+    } else {
+      levels();
+      if (!rc) residual();
+    }
     if (rc) return rc;
   }
   return 0;
@@ -602,14 +645,14 @@ int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *al
   f.q_in = q_in;
   f.q = q_out;
   const int nta = (int)G.tiles_a.size(), ntb = (int)G.tiles_b.size(), nr = (int)G.roots.size();
-  if (alm2map) {
-    if (P->split) rc = run_split(P, true, alm_in, alm_out, q_in, q_out, st);
-    else if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
+  if (P->split) {
+    rc = run_split(P, alm2map, alm_in, alm_out, q_in, q_out, st);
+  } else if (alm2map) {
+    if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
     if (!rc && nr) rc = cuda_check(wm::launch_fast(1, f, fast_grid(P, nr), st), "alm2map level launch");
   } else {
     if (nr) rc = cuda_check(wm::launch_fast(2, f, fast_grid(P, nr), st), "map2alm level launch");
-    if (P->split) rc = rc ? rc : run_split(P, false, alm_in, alm_out, q_in, q_out, st);
-    else if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
+    if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
   }
   if (!rc && P->nslow > 0) {
     wm::LegendreParams p = legendre_params(P);

@@ -86,12 +86,24 @@ struct SplitParams {
   double *q;                      // alm2map: q
   double *xbuf;
   int32_t *status;                // device status word (kStatus*)
+  // level products of depth-1 roots
+  const DevPair *pairs;
+  const int32_t *i32;
+  const DevRootUnit *roots;
+  const DevSplitRoot *sroots;
+  const DevSplitLevelTile *tiles_la, *tiles_lm;
+  int32_t nroots, ntiles_la, ntiles_lm;
+  int8_t *level_a;                // sliced W (A chunks)
+  double2 *level_rs;              // row scales of W
 };
 
-// which: 0 alm operand slices, 1 alm2map residual, 2 X operand slices, 3 map2alm residual
+// which: 0 alm operand slices, 1 alm2map residual, 2 X operand slices, 3 map2alm residual,
+//        4 alm2map level operand (X) slices, 5 alm2map level GEMM,
+//        6 map2alm level operand (q~) slices, 7 map2alm level GEMM
 cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream_t st);
-// Plan creation: P scales of both directions.
+// Plan creation: P scales of both directions, and the sliced W of the levels.
 cudaError_t launch_split_scales(const SplitParams &prm, cudaStream_t st);
+cudaError_t launch_level_slices(const SplitParams &prm, cudaStream_t st);
 
 int legendre_threads();
 cudaError_t launch_legendre(bool alm2map, const LegendreParams &prm, int grid, cudaStream_t st);

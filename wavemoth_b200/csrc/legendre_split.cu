@@ -263,29 +263,55 @@ __global__ void k_split_scales(SplitParams p) {
 }
 
 // ------------------------------------------------------------------------
-// Operand pre-pass: per group, the scale of every vector over the group's K
-// range and the six slices of every K chunk, in the K-major layout of a B
-// operand (kSplitN rows = vectors, kSplitK bytes of K per row).
-//   kAlm = 1: K = group rows, entries a[arow0 + 2 (rs + r)][v0 + v]
-//   kAlm = 0: K = group columns, entries X[row(c)][v0 + v]
-// One CTA of 256 threads per group; thread (v, quarter) handles vector v.
+// Operand pre-pass: per group (or root unit), the scale of every vector over
+// the K range and the six slices of every K chunk, in the K-major layout of
+// a B operand (kSplitN rows = vectors, kSplitK bytes of K per row).
+//   kMode 0: K = group rows, entries a[arow0 + 2 (rs + r)][v0 + v]
+//   kMode 1: K = group columns, entries X[row(c)][v0 + v]
+//   kMode 2: K = s of a root (kT + kB), entries X[inT + s or inB + s - kT]
+//   kMode 3: K = z of a root (n), entries q~[out_left + z]
+// One CTA of 256 threads per group or root; thread (v, quarter) handles v.
 // ------------------------------------------------------------------------
-template <int kAlm>
+template <int kMode>
 __device__ void slice_operand(const SplitParams &p, int gi) {
   __shared__ double red[4][kSplitN];
   __shared__ double2 sc[kSplitN];
-  const DevGroup G = p.groups[gi];
-  const DevSplitGroup S = p.sgroups[gi];
-  const DevMatrix M = p.mats[G.matrix];
   const int v = threadIdx.x & (kSplitN - 1), qtr = threadIdx.x >> 6;
   const int vn = min(kSplitN, p.nvecs - p.v0);
-  const int K = kAlm ? G.nrows : G.ncols;
+  DevGroup G{};
+  DevPair P{};
+  int K, nch;
+  int64_t plane, sidx;
   const double *base;
-  if (kAlm) base = p.alm_in + alm_row0(M, p.lmax) * p.nvecs + p.v0;
-  else base = (G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs : p.xbuf + M.xrow * p.nvecs) + p.v0;
+  if (kMode <= 1) {
+    G = p.groups[gi];
+    const DevSplitGroup S = p.sgroups[gi];
+    const DevMatrix M = p.mats[G.matrix];
+    K = kMode == 0 ? G.nrows : G.ncols;
+    nch = kMode == 0 ? S.nrchunks : S.ncchunks;
+    plane = kMode == 0 ? S.apl : S.xpl;
+    sidx = gi;
+    if (kMode == 0) base = p.alm_in + alm_row0(M, p.lmax) * p.nvecs;
+    else base = G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs : p.xbuf + M.xrow * p.nvecs;
+  } else {
+    const DevRootUnit U = p.roots[gi];
+    const DevSplitRoot R = p.sroots[gi];
+    const DevMatrix M = p.mats[U.matrix];
+    P = p.pairs[U.pair];
+    K = kMode == 2 ? P.kT + P.kB : P.n;
+    nch = kMode == 2 ? R.nsc : R.nzc;
+    plane = kMode == 2 ? R.b_a2m : R.b_m2a;
+    sidx = (int64_t)p.ngroups + gi;
+    base = kMode == 2 ? p.xbuf + M.xrow * p.nvecs : p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs;
+  }
+  base += p.v0;
   auto entry = [&](int k) -> double {
     if (k >= K || v >= vn) return 0.0;
-    const int64_t row = kAlm ? 2 * (int64_t)(G.rs + k) : (int64_t)p.gcols[G.cols + k].row;
+    int64_t row;
+    if (kMode == 0) row = 2 * (int64_t)(G.rs + k);
+    else if (kMode == 1) row = p.gcols[G.cols + k].row;
+    else if (kMode == 2) row = k < P.kT ? P.inT + k : P.inB + (k - P.kT);
+    else row = P.out_left + k;
     return base[row * p.nvecs + v];
   };
   double mx = 0.0;
@@ -295,12 +321,11 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
   if (qtr == 0) {
     const double m4 = fmax(fmax(red[0][v], red[1][v]), fmax(red[2][v], red[3][v]));
     sc[v] = operand_scale(m4);
-    p.vec_scale[(int64_t)gi * kSplitN + v] = sc[v];
+    p.vec_scale[sidx * kSplitN + v] = sc[v];
   }
   __syncthreads();
   const double s = sc[v].x;
-  const int nch = kAlm ? S.nrchunks : S.ncchunks;
-  int8_t *pl = p.planes + (kAlm ? S.apl : S.xpl) * (int64_t)kSplitPlane;
+  int8_t *pl = p.planes + plane * (int64_t)kSplitPlane;
   for (int ch = 0; ch < nch; ++ch) {
     uint32_t w[kSplitSlices][4];
 #pragma unroll
@@ -320,14 +345,22 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
 
 __global__ void __launch_bounds__(256) k_split_operand_alm(SplitParams p) {
   for (int gi = blockIdx.x; gi < p.ngroups; gi += gridDim.x) {
-    slice_operand<1>(p, gi);
+    slice_operand<0>(p, gi);
     __syncthreads();
   }
 }
 
 __global__ void __launch_bounds__(256) k_split_operand_x(SplitParams p) {
   for (int gi = blockIdx.x; gi < p.ngroups; gi += gridDim.x) {
-    slice_operand<0>(p, gi);
+    slice_operand<1>(p, gi);
+    __syncthreads();
+  }
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(256) k_split_operand_level(SplitParams p) {
+  for (int u = blockIdx.x; u < p.nroots; u += gridDim.x) {
+    slice_operand<kMode>(p, u);
     __syncthreads();
   }
 }
@@ -698,6 +731,271 @@ __global__ void __launch_bounds__(kSplitThr, 1) k_m2a_split(SplitParams p) {
 
 }  // namespace
 
+namespace {
+
+// W[z][s] of one interpolation block (k skeleton columns, n rows z): the unit
+// vector of skeleton column s' at its row (filter 0), else column map[z] of
+// the (n - k) x k interpolant (src/butterfly.c.in:222-235).
+__device__ __forceinline__ double w_elem(const int32_t *map, const double *ip_t, int n, int k, int z, int s) {
+  if (z >= n || s >= k) return 0.0;
+  const int mt = map[z];
+  if (mt < 0) return (s == -mt - 1) ? 1.0 : 0.0;
+  return ip_t[mt + (int64_t)s * (n - k)];
+}
+
+// ------------------------------------------------------------------------
+// Plan creation: W of every depth-1 root sliced into A chunks, for both
+// directions (alm2map: rows z, K = s; map2alm: rows s, K = z), with a scale
+// per row.  One CTA of 128 threads per level tile, thread = tile row.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSplitM) k_level_slices(SplitParams p) {
+  const bool a2m = blockIdx.x < p.ntiles_la;
+  const DevSplitLevelTile T = a2m ? p.tiles_la[blockIdx.x] : p.tiles_lm[blockIdx.x - p.ntiles_la];
+  const DevRootUnit U = p.roots[T.unit];
+  const DevPair P = p.pairs[U.pair];
+  const DevSplitRoot R = p.sroots[T.unit];
+  const int K = a2m ? P.kT + P.kB : P.n;
+  const int nk = a2m ? R.nsc : R.nzc;
+  const int r = threadIdx.x, row = T.row0 + r;
+  const bool act = r < T.nrows;
+  const int32_t *mapT = p.i32 + P.mapT, *mapB = p.i32 + P.mapB;
+  const double *ipT = p.f64 + P.ipT_t, *ipB = p.f64 + P.ipB_t;
+  auto w = [&](int k) -> double {
+    if (!act || k >= K) return 0.0;
+    const int z = a2m ? row : k, s = a2m ? k : row;
+    return s < P.kT ? w_elem(mapT, ipT, P.n, P.kT, z, s) : w_elem(mapB, ipB, P.n, P.kB, z, s - P.kT);
+  };
+  double mx = 0.0;
+  for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(w(k)));
+  const double2 sc = operand_scale(mx);
+  if (act) p.level_rs[(a2m ? R.rs_a2m : R.rs_m2a) + row] = sc;
+  int8_t *A = p.level_a + ((a2m ? R.a_a2m : R.a_m2a) + (int64_t)(T.row0 / kSplitM) * nk) * (int64_t)kStageA;
+  for (int c = 0; c < nk; ++c) {
+    for (int h = 0; h < kSplitK / 16; ++h) {
+      double v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = w(c * kSplitK + 16 * h + i);
+      uint32_t wd[kSplitSlices][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        int d[4][kSplitSlices];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) split_digits(v[4 * j + i] * sc.x, d[i]);
+#pragma unroll
+        for (int sl = 0; sl < kSplitSlices; ++sl) wd[sl][j] = pack4(d[0][sl], d[1][sl], d[2][sl], d[3][sl]);
+      }
+      int8_t *dst = A + (int64_t)c * kStageA + (r >> 3) * 512 + h * 128 + (r & 7) * 16;
+#pragma unroll
+      for (int sl = 0; sl < kSplitSlices; ++sl)
+        *reinterpret_cast<uint4 *>(dst + sl * kSliceA) = make_uint4(wd[sl][0], wd[sl][1], wd[sl][2], wd[sl][3]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Level GEMM, split precision.  Unit = one level tile (<= 128 rows of one
+// root's W), K chunks of 64.  Both operands arrive pre-sliced: thread 0
+// copies each chunk with 1D bulk (TMA) copies completing on the stage's
+// mbarrier, two stages, and issues the MMAs; the next tile's first chunk is
+// fetched while the CTA drains the accumulators.
+// ------------------------------------------------------------------------
+constexpr int kLevelThr = 256;
+constexpr int kLevelStage = kStageA + kStageB;  // 73728 bytes
+
+struct LevelSmem {
+  uint64_t full[2], empty[2], acc;
+  uint32_t tmem;
+  int32_t abort;
+};
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+template <bool kA2M>
+struct LevelTile {
+  DevSplitLevelTile T;
+  DevSplitRoot R;
+  int nk;
+  int64_t abase, bbase;
+};
+
+template <bool kA2M>
+__device__ __forceinline__ LevelTile<kA2M> level_tile(const SplitParams &p, int unit) {
+  LevelTile<kA2M> L;
+  L.T = kA2M ? p.tiles_la[unit] : p.tiles_lm[unit];
+  L.R = p.sroots[L.T.unit];
+  L.nk = kA2M ? L.R.nsc : L.R.nzc;
+  L.abase = (kA2M ? L.R.a_a2m : L.R.a_m2a) + (int64_t)(L.T.row0 / kSplitM) * L.nk;
+  L.bbase = kA2M ? L.R.b_a2m : L.R.b_m2a;
+  return L;
+}
+
+// Chunk c of tile L into stage (g & 1) (thread 0): waits for the MMAs that
+// last read the stage (its use g >> 1 - 1), then two bulk copies.
+template <bool kA2M>
+__device__ __forceinline__ bool level_load(const SplitParams &p, unsigned char *smem, LevelSmem *ls,
+                                           const LevelTile<kA2M> &L, int c, long long g) {
+  const int s = (int)(g & 1);
+  const long long use = g >> 1;
+  if (use > 0 && !mbar_wait(&ls->empty[s], (uint32_t)((use - 1) & 1))) return false;
+  const uint32_t dst = smem_u32(smem + s * kLevelStage);
+  expect_tx(&ls->full[s], kLevelStage);
+  bulk_load(dst, p.level_a + (L.abase + c) * (int64_t)kStageA, kStageA, &ls->full[s]);
+  bulk_load(dst + kStageA, p.planes + (L.bbase + c) * (int64_t)kSplitPlane, kStageB, &ls->full[s]);
+  return true;
+}
+
+template <bool kA2M>
+__global__ void __launch_bounds__(kLevelThr, 1) k_level_split(SplitParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  LevelSmem *ls = reinterpret_cast<LevelSmem *>(smem + 2 * kLevelStage);
+  double2 *vsc = reinterpret_cast<double2 *>(smem + 2 * kLevelStage + 128);
+  double2 *rsc = vsc + kSplitN;
+  double *xs = reinterpret_cast<double *>(smem + 2 * kLevelStage + 128 + (kSplitN + kSplitM) * 16);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = kA2M ? p.ntiles_la : p.ntiles_lm;
+  if (warp == 0) tmem_alloc(&ls->tmem);
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&ls->full[s], 1);
+      mbar_init(&ls->empty[s], 1);
+    }
+    mbar_init(&ls->acc, 1);
+    ls->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = ls->tmem;
+  long long g = 0;        // chunks loaded so far (thread 0)
+  uint32_t acc_phase = 0;
+  bool prefetched = false;
+  for (int unit = blockIdx.x; unit < ntiles; unit += gridDim.x) {
+    const LevelTile<kA2M> L = level_tile<kA2M>(p, unit);
+    const DevRootUnit U = p.roots[L.T.unit];
+    const DevPair P = p.pairs[U.pair];
+    const DevMatrix M = p.mats[U.matrix];
+    if (tid < kSplitN) vsc[tid] = p.vec_scale[((int64_t)p.ngroups + L.T.unit) * kSplitN + tid];
+    if (tid < kSplitM)
+      rsc[tid] = tid < L.T.nrows ? p.level_rs[(kA2M ? L.R.rs_a2m : L.R.rs_m2a) + L.T.row0 + tid]
+                                 : make_double2(0.0, 0.0);
+    if (tid == 0) {
+      bool ok = true;
+      long long g0 = g;
+      if (!prefetched) {
+        ok = level_load<kA2M>(p, smem, ls, L, 0, g++);
+      } else {
+        g0 = g - 1;
+      }
+      prefetched = false;
+      for (int c = 0; c < L.nk && ok; ++c) {
+        const long long gc = g0 + c;
+        if (c + 1 < L.nk) ok = level_load<kA2M>(p, smem, ls, L, c + 1, g++);
+        const int s = (int)(gc & 1);
+        if (ok) ok = mbar_wait(&ls->full[s], (uint32_t)((gc >> 1) & 1));
+        if (!ok) break;
+        fence_after_sync();
+        const uint32_t a0 = smem_u32(smem + s * kLevelStage), b0 = a0 + kStageA;
+        for (int ks = 0; ks < kSplitK / 32; ++ks)
+          issue_step(tmem, a0 + ks * 256, b0 + ks * 256, 0, 128, 512, c == 0 && ks == 0);
+        mma_commit(&ls->empty[s]);
+      }
+      if (ok) mma_commit(&ls->acc);
+      else ls->abort = 1;
+    }
+    __syncthreads();
+    if (ls->abort) break;
+    const bool ok = mbar_wait(&ls->acc, acc_phase);
+    acc_phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) ls->abort = 1;
+      break;
+    }
+    fence_after_sync();
+    // prefetch the next tile's first chunk while the accumulators drain
+    if (tid == 0 && unit + (int)gridDim.x < ntiles) {
+      const LevelTile<kA2M> Ln = level_tile<kA2M>(p, unit + gridDim.x);
+      if (Ln.nk > 0) {
+        prefetched = level_load<kA2M>(p, smem, ls, Ln, 0, g++);
+        if (!prefetched) ls->abort = 1;
+      }
+    }
+    // epilogue: TMEM lane = tile row; warps w and w + 4 share a lane quarter
+    {
+      const int row = 32 * (warp & 3) + lane;
+      const double rinv = rsc[row].y;
+      const uint32_t addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+      for (int v8 = (warp >> 2) * 32; v8 < (warp >> 2) * 32 + 32; v8 += 8) {
+        int32_t d[kSplitDiag][8];
+#pragma unroll
+        for (int k = 0; k < kSplitDiag; ++k) tmem_ld8(addr + 64 * k + v8, d[k]);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) xs[row * kXsStride + v8 + j] = recombine(d, j) * rinv * vsc[v8 + j].y;
+      }
+    }
+    fence_before_sync();
+    __syncthreads();
+    {
+      const int vn = min(kSplitN, p.nvecs - p.v0);
+      const int vv = 2 * lane;
+      for (int r = warp; r < L.T.nrows; r += kLevelThr / 32) {
+        const int rr = L.T.row0 + r;
+        double *dst;
+        if (kA2M) {
+          dst = p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs + (int64_t)(P.out_left + rr) * p.nvecs;
+        } else {
+          const int xr = rr < P.kT ? P.inT + rr : P.inB + (rr - P.kT);
+          dst = p.xbuf + (M.xrow + xr) * p.nvecs;
+        }
+        if (vv < vn)
+          *reinterpret_cast<double2 *>(dst + p.v0 + vv) =
+              make_double2(xs[r * kXsStride + vv], xs[r * kXsStride + vv + 1]);
+      }
+    }
+    __syncthreads();
+    if (ls->abort) break;
+  }
+  if (ls->abort) {
+    set_status(p.status, kStatusTimeout);
+    if (tid == 0) {
+      // bounded waits for this CTA's copies and MMAs still in flight
+      for (int s = 0; s < 2; ++s) {
+        const long long gl = (g - 1) - (((g - 1) - s) & 1);  // last chunk loaded into stage s
+        if (gl >= 0) mbar_wait(&ls->full[s], (uint32_t)((gl >> 1) & 1));
+      }
+      mma_commit(&ls->acc);
+      mbar_wait(&ls->acc, acc_phase);
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (warp == 0) tmem_free(tmem);
+}
+
+}  // namespace
+
+static size_t level_smem_bytes() {
+  return (size_t)2 * kLevelStage + 128 + (kSplitN + kSplitM) * 16 + (size_t)kSplitM * kXsStride * 8;
+}
+
+cudaError_t launch_level_slices(const SplitParams &prm, cudaStream_t st) {
+  const int n = prm.ntiles_la + prm.ntiles_lm;
+  if (n == 0) return cudaSuccess;
+  k_level_slices<<<n, kSplitM, 0, st>>>(prm);
+  return cudaGetLastError();
+}
+
 // dynamic shared memory of the split GEMM kernels
 static size_t split_smem_bytes() {
   return (size_t)2 * kStageA + 2 * kStageB + sizeof(SplitSmem) + (kSplitN + kSplitM) * sizeof(double2);
@@ -723,6 +1021,26 @@ cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream
         e = cudaFuncSetAttribute(k_m2a_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         k_m2a_split<<<grid, kSplitThr, sm, st>>>(prm);
+      }
+      break;
+    }
+    case 4:
+      k_split_operand_level<2><<<grid, 256, 0, st>>>(prm);
+      break;
+    case 6:
+      k_split_operand_level<3><<<grid, 256, 0, st>>>(prm);
+      break;
+    case 5:
+    case 7: {
+      const size_t sm = level_smem_bytes();
+      if (which == 5) {
+        e = cudaFuncSetAttribute(k_level_split<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_level_split<true><<<grid, kLevelThr, sm, st>>>(prm);
+      } else {
+        e = cudaFuncSetAttribute(k_level_split<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        k_level_split<false><<<grid, kLevelThr, sm, st>>>(prm);
       }
       break;
     }

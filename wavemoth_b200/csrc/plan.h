@@ -148,6 +148,23 @@ struct DevSplitTileB {  // map2alm: <= kSplitM rows of a group, all its columns
   int32_t group, row0, nrows, pad;
 };
 
+// Split-precision level products of a depth-1 root (T, B) pair, W[z][s] the
+// n x (kT + kB) interpolation matrix with the filter folded in:
+//   alm2map   q[z] = sum_s W[z][s] X[s]     M = z (n), K = s (kT + kB)
+//   map2alm   X[s] = sum_z W[z][s] q~[z]    M = s,     K = z
+// W is sliced once per plan into A chunks laid out as shared memory wants
+// them (kSplitSlices x kSplitM x kSplitK bytes each), per-row scales.
+struct DevSplitRoot {
+  int64_t a_a2m, a_m2a;     // first A chunk of each direction (M tiles x K chunks)
+  int64_t b_a2m, b_m2a;     // first operand-B chunk (X over s, q~ over z)
+  int64_t rs_a2m, rs_m2a;   // first row scale (n rows, kT + kB rows)
+  int32_t nzc, nsc;         // chunks of 64 over z and over s
+};
+
+struct DevSplitLevelTile {  // <= kSplitM rows (z or s) of one root unit
+  int32_t unit, row0, nrows, pad;
+};
+
 // Per ring pair (ring number r from the equator).
 struct DevRing {
   int32_t n;              // pixels in the ring

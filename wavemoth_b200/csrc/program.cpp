@@ -484,6 +484,46 @@ static void build_split_tables(HostProgram &P) {
   for (auto &t : tb) P.stiles_b.push_back(t.second);
   P.split_chunks = std::max(apl, xpl);
   P.split_rows = rows;
+  // level products of the depth-1 roots
+  P.sroots.clear();
+  P.stiles_la.clear();
+  P.stiles_lm.clear();
+  int64_t achunks = 0, lrows = 0, bla = 0, blm = 0;
+  std::vector<std::pair<int32_t, DevSplitLevelTile>> la, lm;
+  for (int32_t u = 0; u < (int32_t)P.roots.size(); ++u) {
+    const DevPair &pr = P.pairs[P.roots[u].pair];
+    const int32_t K = pr.kT + pr.kB;
+    DevSplitRoot R{};
+    R.nzc = (pr.n + kSplitK - 1) / kSplitK;
+    R.nsc = (K + kSplitK - 1) / kSplitK;
+    const int32_t nzt = (pr.n + kSplitM - 1) / kSplitM, nst = (K + kSplitM - 1) / kSplitM;
+    R.a_a2m = achunks;
+    achunks += (int64_t)nzt * R.nsc;
+    R.a_m2a = achunks;
+    achunks += (int64_t)nst * R.nzc;
+    R.b_a2m = bla;
+    bla += R.nsc;
+    R.b_m2a = blm;
+    blm += R.nzc;
+    R.rs_a2m = lrows;
+    lrows += pr.n;
+    R.rs_m2a = lrows;
+    lrows += K;
+    P.sroots.push_back(R);
+    if (R.nsc > 0)
+      for (int32_t z0 = 0; z0 < pr.n; z0 += kSplitM)
+        la.push_back({R.nsc, DevSplitLevelTile{u, z0, std::min(kSplitM, pr.n - z0), 0}});
+    if (R.nzc > 0)
+      for (int32_t s0 = 0; s0 < K; s0 += kSplitM)
+        lm.push_back({R.nzc, DevSplitLevelTile{u, s0, std::min(kSplitM, K - s0), 0}});
+  }
+  std::stable_sort(la.begin(), la.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+  std::stable_sort(lm.begin(), lm.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+  for (auto &t : la) P.stiles_la.push_back(t.second);
+  for (auto &t : lm) P.stiles_lm.push_back(t.second);
+  P.split_level_achunks = achunks;
+  P.split_level_rows = lrows;
+  P.split_chunks = std::max(P.split_chunks, std::max(bla, blm));
 }
 
 bool build_fast_path(HostProgram &P, std::string &err) {

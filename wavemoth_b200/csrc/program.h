@@ -34,8 +34,12 @@ struct HostProgram {
   std::vector<DevSplitGroup> sgroups;   // one per group
   std::vector<DevSplitTileA> stiles_a;
   std::vector<DevSplitTileB> stiles_b;
-  int64_t split_chunks = 0;             // operand chunks of the larger direction
+  int64_t split_chunks = 0;             // operand-B chunks of the largest use
   int64_t split_rows = 0;               // row scales (sum of group rows)
+  std::vector<DevSplitRoot> sroots;     // one per root unit
+  std::vector<DevSplitLevelTile> stiles_la, stiles_lm;  // alm2map / map2alm level tiles
+  int64_t split_level_achunks = 0;      // A chunks of W, both directions
+  int64_t split_level_rows = 0;         // row scales of W, both directions
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)
