@@ -58,6 +58,7 @@ namespace wm {
 
 namespace {
 
+constexpr int kRadixLog = 4;           // largest pass radix 2^kRadixLog
 constexpr int kRingThreads = 256;      // class 0: <= 4096 complex per CTA
 constexpr int kRingThreadsWide = 512;  // class 1: <= 8192 complex per CTA
 constexpr int kPhaseLo = 64;           // e^{i m phi0} = hi[m / 64] * lo[m % 64]
@@ -198,8 +199,13 @@ __device__ __forceinline__ void fft_pass_r(int R, int M, int len, int lg, const 
   switch (R) {
     case 2: fft_pass<2, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
     case 4: fft_pass<4, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
-    case 8: fft_pass<8, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
-    default: fft_pass<16, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    case 8:
+      if (kRadixLog > 3) {
+        fft_pass<8, SIGN, DIF>(M, len, lg, tw, twlen, load, store);
+        break;
+      }
+      [[fallthrough]];
+    default: fft_pass<(1 << kRadixLog), SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
   }
 }
 
@@ -244,8 +250,13 @@ __device__ __forceinline__ void bluestein_mid(int R, int M, int lg, const cplx *
   switch (R) {
     case 2: bluestein_mid_r<2>(M, lg, F, fsign, tw, twlen, load, store); break;
     case 4: bluestein_mid_r<4>(M, lg, F, fsign, tw, twlen, load, store); break;
-    case 8: bluestein_mid_r<8>(M, lg, F, fsign, tw, twlen, load, store); break;
-    default: bluestein_mid_r<16>(M, lg, F, fsign, tw, twlen, load, store); break;
+    case 8:
+      if (kRadixLog > 3) {
+        bluestein_mid_r<8>(M, lg, F, fsign, tw, twlen, load, store);
+        break;
+      }
+      [[fallthrough]];
+    default: bluestein_mid_r<(1 << kRadixLog)>(M, lg, F, fsign, tw, twlen, load, store); break;
   }
 }
 
@@ -253,13 +264,13 @@ __device__ __forceinline__ void bluestein_mid(int R, int M, int lg, const cplx *
 // above 1) then 16s.  DIT runs them in reverse order.
 struct Radices {
   int n;         // number of passes
-  int r[5];      // radix of DIF pass p
-  int len[5];    // block length of DIF pass p (the DIT pass mirroring it has the same)
+  int r[8];      // radix of DIF pass p
+  int len[8];    // block length of DIF pass p (the DIT pass mirroring it has the same)
 };
 
 __device__ __forceinline__ Radices radices(int M) {
   Radices s;
-  const int lgM = ilog2(M), r0 = lgM & 3;
+  const int lgM = ilog2(M), r0 = lgM % kRadixLog;
   s.n = 0;
   int len = M;
   if (r0) {
@@ -267,10 +278,10 @@ __device__ __forceinline__ Radices radices(int M) {
     s.len[s.n++] = len;
     len >>= r0;
   }
-  for (int k = 0; k < (lgM >> 2); ++k) {
-    s.r[s.n] = 16;
+  for (int k = 0; k < lgM / kRadixLog; ++k) {
+    s.r[s.n] = 1 << kRadixLog;
     s.len[s.n++] = len;
-    len >>= 4;
+    len >>= kRadixLog;
   }
   return s;
 }
@@ -369,7 +380,7 @@ __device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mm
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? 2 : 1)
+__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog == 4 ? 2 : 3) : 1)
     k_ring_synthesis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, task0 + blockIdx.x);
@@ -455,7 +466,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? 2 : 1)
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? 2 : 1)
+__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog == 4 ? 2 : 3) : 1)
     k_ring_analysis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, task0 + blockIdx.x);
