@@ -66,6 +66,26 @@ int wavemoth_execute_alm2map_device(wavemoth_plan plan, const double *alm, doubl
 int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, double *alm,
                                     void *stream);
 
+/* Batches of uneven transforms as one CUDA graph launch.  New; the
+   reference executes one plan at a time (src/wavemoth.c:1271-1283).
+   Request i runs plans[i] in directions[i] (0 alm2map, 1 map2alm) from the
+   device buffer inputs[i] into outputs[i]; the plans may differ in nside,
+   lmax, nmaps and precision, but no two requests may share a plan.  At
+   creation waits for `stream`, captures the requests, longest first, onto
+   1, 2, 4 or 8 (at most max_width; <= 0 for 8) parallel graph branches,
+   times each graph on a private stream (this runs every request a few
+   times) and keeps the fastest.  Creation must not run inside another
+   stream capture. */
+typedef struct _wavemoth_batch *wavemoth_batch;
+wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const int *directions,
+                                     const double *const *inputs, double *const *outputs,
+                                     int max_width, void *stream);
+/* One graph launch of every request of the batch on `stream`. */
+int wavemoth_batch_execute(wavemoth_batch batch, void *stream);
+/* The branch count the creation chose and its measured time per launch. */
+int wavemoth_batch_info(wavemoth_batch batch, int *width, double *ms);
+void wavemoth_batch_destroy(wavemoth_batch batch);
+
 /* The alm2map Legendre step of `plan` (q = A^T a for every (m, parity)),
    for callers that cannot allocate device memory when they run it (inside a
    custom allocator's callback, under a framework that owns all device

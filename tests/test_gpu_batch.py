@@ -1,0 +1,78 @@
+"""Uneven batches in one graph launch (wavemoth_b200.batch): requests of
+different nside, lmax = 2 nside, 1..8 maps, both directions and both
+precisions.  Each request's output must equal (bitwise) the output of the
+same transform called alone, on two launches in a row; the split-precision
+requests are also checked against the oracle's butterfly transform at the
+split tolerance (max |error| <= 1e-9 max |value|).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import sht as osht
+
+from .plans import plan_file
+
+pytestmark = pytest.mark.gpu
+
+
+def _transform(nside, nmaps, precision):
+    from wavemoth_b200.sht import Transform
+    lmax = 2 * nside
+    return Transform(plan_file(nside, lmax, 16, 1e-10, 20.0), nside, lmax, nmaps, precision=precision)
+
+
+def test_uneven_batch_matches_single_calls():
+    from wavemoth_b200.batch import Batch
+    rng = np.random.default_rng(55)
+    specs = [(nside, int(rng.integers(1, 9)), prec, direction)
+             for nside, prec, direction in [(8, "split", "alm2map"), (16, "double", "alm2map"),
+                                            (32, "split", "alm2map"), (16, "split", "map2alm"),
+                                            (8, "double", "map2alm"), (32, "double", "alm2map"),
+                                            (64, "split", "alm2map")]]
+    reqs, singles, alms = [], [], []
+    for i, (nside, nmaps, prec, direction) in enumerate(specs):
+        T = _transform(nside, nmaps, prec)
+        if direction == "alm2map":
+            a = osht.random_alm(T.lmax, nmaps, seed=600 + i)
+            inp = torch.from_numpy(a).cuda()
+            out = torch.empty((T.npix, nmaps), dtype=torch.float64, device="cuda")
+            single = T.alm2map(inp).clone()
+        else:
+            a = rng.standard_normal((T.npix, nmaps))
+            inp = torch.from_numpy(a).cuda()
+            out = torch.empty((T.nalm, nmaps), dtype=torch.complex128, device="cuda")
+            single = T.map2alm(inp).clone()
+        alms.append(a)
+        reqs.append((T, direction, inp, out))
+        singles.append(single)
+    B = Batch(reqs)
+    width, ms = B.info()
+    assert width in (1, 2, 4, 8) and ms > 0
+    for _ in range(2):
+        for r in reqs:
+            r[3].zero_()
+        B.execute()
+        torch.cuda.synchronize()
+        for r, s in zip(reqs, singles):
+            assert torch.equal(r[3], s)
+    for (nside, nmaps, prec, direction), (T, _, _, out), a in zip(specs, reqs, alms):
+        T.device_status()
+        if prec == "split" and direction == "alm2map":
+            path = plan_file(nside, 2 * nside, 16, 1e-10, 20.0)
+            want = osht.alm2map_butterfly(osht.Rev1File(path), a, 2 * nside)
+            got = out.cpu().numpy()
+            assert np.abs(got - want).max() <= 1e-9 * np.abs(want).max()
+    B.close()
+    for r in reqs:
+        r[0].close()
+
+
+def test_batch_rejects_shared_transform():
+    from wavemoth_b200.batch import Batch
+    T = _transform(8, 1, "double")
+    a = torch.from_numpy(osht.random_alm(16, 1, seed=1)).cuda()
+    m = torch.empty((T.npix, 1), dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        Batch([(T, "alm2map", a, m), (T, "alm2map", a, m)])
+    T.close()

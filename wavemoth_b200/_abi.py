@@ -23,6 +23,10 @@ SIGNATURES = {
     "wavemoth_last_error": (ctypes.c_char_p, []),
     "wavemoth_plan_status": (ctypes.c_int, [_vp]),
     "wavemoth_plan_device_status": (ctypes.c_int, [_vp, _vp]),
+    "wavemoth_batch_create": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "wavemoth_batch_execute": (ctypes.c_int, [_vp, _vp]),
+    "wavemoth_batch_info": (ctypes.c_int, [_vp, _vp, _vp]),
+    "wavemoth_batch_destroy": (None, [_vp]),
     "wavemoth_execute_alm2map_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_execute_map2alm_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_get_work": (ctypes.c_int, [_vp, _dp]),

@@ -1,0 +1,208 @@
+// Batches of transforms of uneven size executed as one CUDA graph launch.
+//
+// A batch holds requests (plan, direction, device input, device output) of
+// any nside / lmax / number of maps.  At creation the requests are captured
+// into one CUDA graph: they are ordered by their algorithmic work (Legendre
+// flops plus ring bytes, from wavemoth_plan_work) and assigned longest first
+// to the least-loaded of `width` parallel capture branches, so that small
+// transforms fill the SMs that large ones leave idle.  The width is
+// autotuned: a graph is built and timed for every width in {1, 2, 4, 8}
+// (at most the number of requests) and the fastest is kept.  Every
+// execute is then one cudaGraphLaunch.
+//
+// The plans' own buffers (q, X, operand slices) are shared by all calls on
+// one plan, so a batch must not hold two requests on the same plan.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "wavemoth.h"
+#include "wavemoth_b200.h"
+
+namespace wm {
+int set_last_error(int code, const std::string &msg);
+}
+
+struct _wavemoth_batch {
+  struct Req {
+    wavemoth_plan plan;
+    int direction;
+    const double *in;
+    double *out;
+    double cost;
+  };
+  std::vector<Req> reqs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int width = 0;
+  double ms = 0.0;
+
+  ~_wavemoth_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+namespace {
+
+int cuda_err(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return 0;
+  return wm::set_last_error(WAVEMOTH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Captures the batch with `width` branches forked from `origin`.
+int capture(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGraph_t *out) {
+  std::vector<cudaStream_t> br(width, nullptr);
+  std::vector<cudaEvent_t> done(width, nullptr);
+  cudaEvent_t fork = nullptr;
+  int rc = cuda_err(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "batch event");
+  for (int i = 0; i < width && !rc; ++i) {
+    rc = cuda_err(cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking), "batch stream");
+    if (!rc) rc = cuda_err(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "batch event");
+  }
+  bool capturing = false;
+  if (!rc) {
+    rc = cuda_err(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal), "begin capture");
+    capturing = !rc;
+  }
+  if (!rc) rc = cuda_err(cudaEventRecord(fork, origin), "fork");
+  for (int i = 0; i < width && !rc; ++i) rc = cuda_err(cudaStreamWaitEvent(br[i], fork, 0), "fork");
+  // longest first onto the least-loaded branch
+  std::vector<double> load(width, 0.0);
+  for (const auto &r : B.reqs) {
+    if (rc) break;
+    const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[b] += r.cost;
+    rc = r.direction == 0 ? wavemoth_execute_alm2map_device(r.plan, r.in, r.out, br[b])
+                          : wavemoth_execute_map2alm_device(r.plan, r.in, r.out, br[b]);
+  }
+  for (int i = 0; i < width && !rc; ++i) {
+    rc = cuda_err(cudaEventRecord(done[i], br[i]), "join");
+    if (!rc) rc = cuda_err(cudaStreamWaitEvent(origin, done[i], 0), "join");
+  }
+  if (capturing) {
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(origin, &g);
+    if (!rc) rc = cuda_err(e, "end capture");
+    if (rc && g) cudaGraphDestroy(g);
+    if (!rc) *out = g;
+  }
+  for (int i = 0; i < width; ++i) {
+    if (br[i]) cudaStreamDestroy(br[i]);
+    if (done[i]) cudaEventDestroy(done[i]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  return rc;
+}
+
+// Mean time of `reps` launches of an instantiated graph (after one warm-up).
+int time_graph(cudaGraphExec_t ex, cudaStream_t st, int reps, double *ms) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = cuda_err(cudaEventCreate(&a), "timing event");
+  if (!rc) rc = cuda_err(cudaEventCreate(&b), "timing event");
+  if (!rc) rc = cuda_err(cudaGraphLaunch(ex, st), "graph launch");
+  if (!rc) rc = cuda_err(cudaEventRecord(a, st), "timing event");
+  for (int i = 0; i < reps && !rc; ++i) rc = cuda_err(cudaGraphLaunch(ex, st), "graph launch");
+  if (!rc) rc = cuda_err(cudaEventRecord(b, st), "timing event");
+  if (!rc) rc = cuda_err(cudaEventSynchronize(b), "timing event");
+  float t = 0.f;
+  if (!rc) rc = cuda_err(cudaEventElapsedTime(&t, a, b), "timing event");
+  if (!rc) *ms = t / reps;
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const int *directions,
+                                     const double *const *inputs, double *const *outputs, int max_width,
+                                     void *stream) {
+  if (nreq <= 0 || !plans || !directions || !inputs || !outputs) {
+    wm::set_last_error(WAVEMOTH_ERR_ARG, "invalid batch arguments");
+    return nullptr;
+  }
+  auto *B = new _wavemoth_batch();
+  for (int i = 0; i < nreq; ++i) {
+    if (!plans[i] || !inputs[i] || !outputs[i] || (directions[i] != 0 && directions[i] != 1)) {
+      wm::set_last_error(WAVEMOTH_ERR_ARG, "batch request " + std::to_string(i) + " is invalid");
+      delete B;
+      return nullptr;
+    }
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) {
+        wm::set_last_error(WAVEMOTH_ERR_ARG, "two batch requests share one plan (its buffers would race)");
+        delete B;
+        return nullptr;
+      }
+    double w[12] = {0};
+    if (wavemoth_plan_work(plans[i], wavemoth_plan_nmaps(plans[i]), w) != 0) {
+      delete B;
+      return nullptr;
+    }
+    // seconds-scale estimate: FP64 flops at 30 TF/s plus ring bytes at 1 TB/s
+    const double cost = w[0] / 30e12 + w[3] / 1e12;
+    B->reqs.push_back({plans[i], directions[i], inputs[i], outputs[i], cost});
+  }
+  std::stable_sort(B->reqs.begin(), B->reqs.end(),
+                   [](const _wavemoth_batch::Req &a, const _wavemoth_batch::Req &b) { return a.cost > b.cost; });
+  // capture and timing run on a private stream (the legacy default stream
+  // cannot be captured); the caller's pending work is waited for first
+  cudaStream_t st = nullptr;
+  if (cuda_err(cudaStreamSynchronize((cudaStream_t)stream), "batch create") ||
+      cuda_err(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "batch stream")) {
+    delete B;
+    return nullptr;
+  }
+  const int wmax = std::max(1, std::min(std::min(nreq, 8), max_width > 0 ? max_width : 8));
+  for (int width = 1; width <= wmax; width *= 2) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    int rc = capture(*B, width, st, &g);
+    if (!rc) rc = cuda_err(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
+    double ms = 0.0;
+    if (!rc) rc = time_graph(ex, st, 3, &ms);
+    if (rc) {
+      if (ex) cudaGraphExecDestroy(ex);
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(st);
+      delete B;
+      return nullptr;
+    }
+    if (!B->exec || ms < B->ms) {
+      if (B->exec) cudaGraphExecDestroy(B->exec);
+      if (B->graph) cudaGraphDestroy(B->graph);
+      B->exec = ex;
+      B->graph = g;
+      B->width = width;
+      B->ms = ms;
+    } else {
+      cudaGraphExecDestroy(ex);
+      cudaGraphDestroy(g);
+    }
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return B;
+}
+
+int wavemoth_batch_execute(wavemoth_batch batch, void *stream) {
+  if (!batch || !batch->exec) return wm::set_last_error(WAVEMOTH_ERR_ARG, "NULL batch");
+  return cuda_err(cudaGraphLaunch(batch->exec, (cudaStream_t)stream), "batch launch");
+}
+
+int wavemoth_batch_info(wavemoth_batch batch, int *width, double *ms) {
+  if (!batch) return wm::set_last_error(WAVEMOTH_ERR_ARG, "NULL batch");
+  if (width) *width = batch->width;
+  if (ms) *ms = batch->ms;
+  return 0;
+}
+
+void wavemoth_batch_destroy(wavemoth_batch batch) { delete batch; }
+
+}  // extern "C"
