@@ -250,6 +250,29 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def int8_peak_tops(torch):
+    """Dense int8 tensor throughput of this GPU (cuBLASLt through
+    torch._int_mm, 8192^3), or None if unavailable."""
+    try:
+        n = 8192
+        a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device="cuda")
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b
+        return 2.0 * n ** 3 / best / 1e12
+    except Exception:
+        return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -257,6 +280,15 @@ def measured_peaks():
             d = json.load(f)
         return d.get("hbm_gbs"), "measured"
     return 6650.0, "fallback"
+
+
+def measured_peaks_bf16():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("bf16_tflops", 1590.0))
+    return 1590.0
 
 
 def profile_traffic(kernel):
@@ -404,22 +436,35 @@ def run_b200(a):
     peak_hbm, hbm_src = measured_peaks()
     if dominant.startswith("legendre"):
         fp64 = fp64_peak_tflops(torch)
-        achieved = work["legendre_flops"] / (kms[dominant] / 1e3) / 1e12
-        roofline = {"bound": "fp64", "kernel": dominant, "achieved": achieved, "peak": fp64,
-                    "unit": "TFLOP/s", "frac": achieved / fp64,
-                    "peak_source": "cuBLAS DGEMM 8192^3 measured by bench.py on this GPU "
-                                   "(FP64 is not in MEASURED_PEAKS.json)",
-                    "traffic": profile_traffic(dominant),
-                    "algorithmic_flops_per_launch": work["legendre_flops"],
-                    "matrix_bytes_per_launch": work["matrix_bytes"],
-                    "hbm_view": {"achieved_gbs": (work["matrix_bytes"] + work["legendre_vector_bytes"])
-                                 / (kms[dominant] / 1e3) / 1e9,
-                                 "peak_gbs": peak_hbm, "peak_source": hbm_src}}
+        fp64_achieved = work["legendre_flops"] / (kms[dominant] / 1e3) / 1e12
+        fp64_view = {"achieved": fp64_achieved, "peak": fp64, "unit": "TFLOP/s", "frac": fp64_achieved / fp64,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured by bench.py on this GPU",
+                     "what": "algorithmic FP64 flops of the transform (2 per multiply-add of 64 vectors, "
+                             "5 per recurrence step) over the phase time"}
+        if a.precision == "split":
+            ops = work["split_int8_ops_" + ("alm2map" if dominant.endswith("alm2map") else "map2alm")]
+            achieved = ops / (kms[dominant] / 1e3) / 1e12
+            peak = int8_peak_tops(torch)
+            src = "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured by bench.py on this GPU"
+            if peak is None:
+                peak, src = 2.0 * measured_peaks_bf16(), "2 x MEASURED_PEAKS.json dense bf16 (int8 rate)"
+            roofline = {"bound": "tensor", "kernel": dominant + " (split: residual + level int8 GEMMs)",
+                        "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)", "frac": achieved / peak,
+                        "peak_source": src, "traffic": profile_traffic(dominant),
+                        "int8_ops_per_launch": ops, "fp64_equivalent": fp64_view}
+        else:
+            roofline = {"bound": "tensor", "kernel": dominant + " (FP64 DMMA)", "achieved": fp64_achieved,
+                        "peak": fp64, "unit": "TFLOP/s (fp64)", "frac": fp64_achieved / fp64,
+                        "peak_source": fp64_view["peak_source"], "traffic": profile_traffic(dominant),
+                        "algorithmic_flops_per_launch": work["legendre_flops"]}
+        roofline["hbm_view"] = {"achieved_gbs": (work["matrix_bytes"] + work["legendre_vector_bytes"])
+                                / (kms[dominant] / 1e3) / 1e9, "peak_gbs": peak_hbm, "peak_source": hbm_src}
     else:
         achieved = work["ring_bytes"] / (kms[dominant] / 1e3) / 1e9
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_hbm,
                     "unit": "GB/s", "frac": achieved / peak_hbm, "peak_source": hbm_src,
-                    "traffic": profile_traffic(dominant)}
+                    "traffic": profile_traffic(dominant),
+                    "algorithmic_bytes_per_launch": work["ring_bytes"]}
     roofline["kernel_ms_per_launch"] = kms
     roofline["kernel_time_share"] = share
 

@@ -139,7 +139,8 @@ int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out);
    and for the split-precision residual products (out needs 12 entries):
    out[8] / out[9] elements of P generated by the alm2map / map2alm tiles
    per pass of 64 vectors (zero padding of the tiles included), out[10] /
-   out[11] int8 tensor-core operations of one alm2map / map2alm launch. */
+   out[11] int8 tensor-core operations of one alm2map / map2alm launch
+   (residual and level GEMMs). */
 int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out);
 
 /* Parses and validates a rev1 file for (Nside, lmax) exactly as plan

@@ -924,17 +924,18 @@ int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out) {
   out[7] = (double)plan->grid;
   // split path: 64-row (or 64-column) K chunks of 128-row M tiles; per K
   // step of 32, nine MMAs with N summing to 1664 (six slices, i + j <= 6)
-  double ea = 0.0, eb = 0.0;
+  double ea = 0.0, eb = 0.0, la = 0.0, lb = 0.0;
   for (const auto &T : G.stiles_a) ea += (double)(G.sgroups[T.group].nrchunks - T.kc0);
   for (const auto &T : G.stiles_b) eb += (double)G.sgroups[T.group].ncchunks;
-  ea *= (double)wm::kSplitM * wm::kSplitK;
-  eb *= (double)wm::kSplitM * wm::kSplitK;
+  for (const auto &T : G.stiles_la) la += (double)G.sroots[T.unit].nsc;
+  for (const auto &T : G.stiles_lm) lb += (double)G.sroots[T.unit].nzc;
+  const double chunk = (double)wm::kSplitM * wm::kSplitK;
   const double passes = (double)((2 * nmaps + wm::kSplitN - 1) / wm::kSplitN);
-  const double ops_per_elem = 2.0 * 1664.0;  // per element of P (M x K), all slice windows
-  out[8] = ea;
-  out[9] = eb;
-  out[10] = ea * ops_per_elem * passes;
-  out[11] = eb * ops_per_elem * passes;
+  const double ops_per_elem = 2.0 * 1664.0;  // per element of an A chunk (M x K), all slice windows
+  out[8] = ea * chunk;
+  out[9] = eb * chunk;
+  out[10] = (ea + la) * chunk * ops_per_elem * passes;
+  out[11] = (eb + lb) * chunk * ops_per_elem * passes;
   return 0;
 }
 
