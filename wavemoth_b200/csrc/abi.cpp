@@ -227,17 +227,22 @@ RingTable ring_table(int nside, int nmaps, int mmax) {
       T.twlen = std::max(T.twlen, 2 * N);  // roots e^{2 pi i k / n}, n = 2N
     }
     T.rings[r] = R;
-    int G = 1, cls = 1;
-    if (len <= wm::kRingBufferCplx) {
+    // both hemispheres in one CTA (lanes = sides x maps) when they fit a
+    // class; the longest transforms run one hemisphere at a time
+    int G = 1, cls = 1, two = 1;
+    if (2 * len <= wm::kRingBufferCplx) {
       cls = 0;
-      G = std::min(gmax, wm::kRingBufferCplx / len);
+      G = std::min(gmax, wm::kRingBufferCplx / (2 * len));
+    } else if (2 * len > 2 * wm::kRingBufferCplx) {
+      two = 0;
     }
     int lg = 0;
     while ((1 << lg) < G) ++lg;
-    const double cost = (double)G * len * (R.bluestein_m ? 2.5 : 1.0) + (double)G * (mmax + 1);
-    T.max_cta_cplx = std::max(T.max_cta_cplx, (int64_t)G * len);
+    const int64_t cplx = (int64_t)G * len << two;
+    const double cost = (double)cplx * (R.bluestein_m ? 2.5 : 1.0) + (double)G * (mmax + 1);
+    T.max_cta_cplx = std::max(T.max_cta_cplx, cplx);
     for (int g0 = 0; g0 < nmaps; g0 += G)
-      items.push_back({cost, wm::DevRingTask{r, g0, lg, 0}, cls, (int64_t)G * len});
+      items.push_back({cost, wm::DevRingTask{r, g0, lg, two}, cls, cplx});
   }
   std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
     return a.cls != b.cls ? a.cls < b.cls : a.cost > b.cost;

@@ -177,12 +177,13 @@ struct DevRing {
   int64_t aux;            // Bluestein: complex offset of chirp[n/2] then root[n/2 + 1]
 };
 
-// One CTA of a ring kernel: ring pair `ring`, maps [map0, map0 + 2^lg).
+// One CTA of a ring kernel: ring pair `ring`, maps [map0, map0 + 2^lg), both
+// hemispheres at once if `two` (else one after the other).
 struct DevRingTask {
   int32_t ring;
   int32_t map0;
   int32_t lg;
-  int32_t pad;
+  int32_t pad;   // two
 };
 
 // Device-resident error word (never trap: kernels record and return).

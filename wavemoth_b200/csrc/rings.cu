@@ -336,7 +336,11 @@ __device__ __forceinline__ cplx phase_at(const cplx *lo, const cplx *hi, int m) 
 
 struct RingCta {
   DevRing R;
-  int ring, map0, lg, nm;  // nm: maps of the group that exist
+  int ring, map0;
+  int lgm;   // log2 of the maps per CTA
+  int two;   // 1: both hemispheres in the CTA (lane g = side * 2^lgm + map)
+  int lg;    // log2 of the lanes: lgm + two
+  int nm;    // maps of the group that exist
   int n, N, M, bits;
   bool pow2;
 };
@@ -347,7 +351,9 @@ __device__ __forceinline__ RingCta ring_cta(const RingParams &p, int task) {
   c.R = p.rings[T.ring];
   c.ring = T.ring;
   c.map0 = T.map0;
-  c.lg = T.lg;
+  c.lgm = T.lg;
+  c.two = T.pad;
+  c.lg = T.lg + T.pad;
   c.nm = min(1 << T.lg, p.nmaps - T.map0);
   c.n = c.R.n;
   c.N = c.n >> 1;
@@ -357,26 +363,36 @@ __device__ __forceinline__ RingCta ring_cta(const RingParams &p, int task) {
   return c;
 }
 
-// W[j] of one map (q row pointer `qg` at ring r, map g), aliasing sum in increasing m
-__device__ __forceinline__ cplx alias_sum(const double *qg, int j, int n, int mmax, int64_t qstride,
-                                          int64_t half, double sgn, const cplx *plo, const cplx *phi) {
-  cplx acc = {0.0, 0.0};
+// Lane g of a CTA: its map (within the group) and hemisphere (0 north, 1
+// south); `side` is the hemisphere of a CTA that runs them one at a time.
+__device__ __forceinline__ int lane_map(const RingCta &c, int g) { return g & ((1 << c.lgm) - 1); }
+__device__ __forceinline__ int lane_side(const RingCta &c, int g, int side) { return c.two ? g >> c.lgm : side; }
+__device__ __forceinline__ bool lane_live(const RingCta &c, int g, int side) {
+  return lane_map(c, g) < c.nm && !(lane_side(c, g, side) == 1 && c.ring == 0);
+}
+
+// Even and odd partial sums of W[j] of one map (q row pointer `qg` at ring r,
+// map g): W = A + B on the northern ring, A - B on the southern one; the
+// aliasing sum runs in increasing m.
+__device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int mmax, int64_t qstride,
+                                           int64_t half, const cplx *plo, const cplx *phi, cplx &A, cplx &B) {
+  A = {0.0, 0.0};
+  B = {0.0, 0.0};
   for (int base = 0;; base += n) {
     const int m1 = base + j;
     if (m1 > mmax) break;
     {
-      const cplx e = ld2(qg + m1 * qstride), o = ld2(qg + m1 * qstride + half);
-      const cplx t = {e.x + sgn * o.x, e.y + sgn * o.y};
-      acc = cadd(acc, cmul(t, phase_at(plo, phi, m1)));
+      const cplx ph = phase_at(plo, phi, m1);
+      A = cadd(A, cmul(ld2(qg + m1 * qstride), ph));
+      B = cadd(B, cmul(ld2(qg + m1 * qstride + half), ph));
     }
     const int m2 = base + n - j;
     if (m2 <= mmax) {
-      const cplx e = ld2(qg + m2 * qstride), o = ld2(qg + m2 * qstride + half);
-      const cplx t = {e.x + sgn * o.x, e.y + sgn * o.y};
-      acc = cadd(acc, cconj(cmul(t, phase_at(plo, phi, m2))));
+      const cplx ph = phase_at(plo, phi, m2);
+      A = cadd(A, cconj(cmul(ld2(qg + m2 * qstride), ph)));
+      B = cadd(B, cconj(cmul(ld2(qg + m2 * qstride + half), ph)));
     }
   }
-  return acc;
 }
 
 template <int THREADS>
@@ -395,53 +411,65 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
   const Radices rs = radices(M);
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
-  for (int side = 0; side < 2; ++side) {
+  const int gmm = (1 << c.lgm) - 1;
+  for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;  // the equator is written once
-    const double sgn = side ? -1.0 : 1.0;
-    // Z[k] and Z[N - k] (natural order, chirped for Bluestein rings) from
-    // W[k] and W[N - k]
+    // Z[k] and Z[N - k] (natural order, chirped for Bluestein rings) of the
+    // CTA's hemispheres, from W[k] and W[N - k]
     const int npairs = (N >> 1) + 1;
-    for (int t = threadIdx.x; t < (npairs << lg); t += blockDim.x) {
-      const int g = t & gm, kk = t >> lg, kr = N - kk;
-      cplx Wa = {0.0, 0.0}, Wb = {0.0, 0.0};  // W[kk], W[N - kk]
-      if (g < c.nm) {
-        const double *qg = qbase + 2 * g;
-        Wa = alias_sum(qg, kk, n, p.mmax, qstride, half, sgn, plo, phi);
-        Wb = kr == kk ? Wa : alias_sum(qg, kr, n, p.mmax, qstride, half, sgn, plo, phi);
+    for (int t = threadIdx.x; t < (npairs << c.lgm); t += blockDim.x) {
+      const int mi = t & gmm, kk = t >> c.lgm, kr = N - kk;
+      cplx Aa = {0.0, 0.0}, Ba = {0.0, 0.0}, Ab = {0.0, 0.0}, Bb = {0.0, 0.0};  // at kk and N - kk
+      if (mi < c.nm) {
+        const double *qg = qbase + 2 * mi;
+        alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, Aa, Ba);
+        if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, Ab, Bb);
+        else { Ab = Aa; Bb = Ba; }
       }
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int k = e ? kr : kk;
-        if (e && (kr == kk || kr == N)) break;
-        cplx Wk = e ? Wb : Wa, Wc = cconj(e ? Wa : Wb);
-        if (k == 0) {
-          Wk.y = 0.0;
-          Wc.y = 0.0;
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && !c.two) break;
+        const int sd = c.two ? h : side;
+        const double sgn = sd ? -1.0 : 1.0;
+        const int g = (h << c.lgm) | mi;
+        const cplx Wa = {Aa.x + sgn * Ba.x, Aa.y + sgn * Ba.y}, Wb = {Ab.x + sgn * Bb.x, Ab.y + sgn * Bb.y};
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int k = e ? kr : kk;
+          if (e && (kr == kk || kr == N)) break;
+          cplx Wk = e ? Wb : Wa, Wc = cconj(e ? Wa : Wb);
+          if (k == 0) {
+            Wk.y = 0.0;
+            Wc.y = 0.0;
+          }
+          const cplx sm = cadd(Wk, Wc), d = csub(Wk, Wc);
+          const cplx Z = cadd(sm, mul_i(cmul(ring_root(p, c.R, k), d)));
+          buf[at(k, g, lg)] = c.pow2 ? Z : cmul(Z, ring_chirp(p, c.R, k));
         }
-        const cplx sm = cadd(Wk, Wc), d = csub(Wk, Wc);
-        const cplx Z = cadd(sm, mul_i(cmul(ring_root(p, c.R, k), d)));
-        buf[at(k, g, lg)] = c.pow2 ? Z : cmul(Z, ring_chirp(p, c.R, k));
       }
     }
     if (!c.pow2)
       for (int t = threadIdx.x; t < ((M - N) << lg); t += blockDim.x)
         buf[at(N + (t >> lg), t & gm, lg)] = {0.0, 0.0};
     __syncthreads();
-    double *out = p.map + (side ? c.R.off_south : c.R.off_north) * p.nmaps + c.map0;
     auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, lg)]; };
     auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, lg)] = v; };
+    auto out_row = [&](int g, int64_t pix) -> double * {
+      const int64_t off = lane_side(c, g, side) ? c.R.off_south : c.R.off_north;
+      return p.map + (off + pix) * p.nmaps + c.map0 + lane_map(c, g);
+    };
     // pixels 2s, 2s + 1 of output z[s]; power of two: DIF position pos holds z[bitrev(pos)]
     auto pix_dif = [&](int pos, int g, cplx z) {
-      if (g >= c.nm) return;
-      const int64_t s = bitrev((unsigned)pos, c.bits);
-      out[(2 * s) * p.nmaps + g] = z.x;
-      out[(2 * s + 1) * p.nmaps + g] = z.y;
+      if (!lane_live(c, g, side)) return;
+      const int64_t s2 = 2 * (int64_t)bitrev((unsigned)pos, c.bits);
+      *out_row(g, s2) = z.x;
+      *out_row(g, s2 + 1) = z.y;
     };
     auto pix_blue = [&](int k, int g, cplx z) {
-      if (k >= N || g >= c.nm) return;
+      if (k >= N || !lane_live(c, g, side)) return;
       z = cscale(cmul(z, ring_chirp(p, c.R, k)), inv);
-      out[(2 * (int64_t)k) * p.nmaps + g] = z.x;
-      out[(2 * (int64_t)k + 1) * p.nmaps + g] = z.y;
+      *out_row(g, 2 * (int64_t)k) = z.x;
+      *out_row(g, 2 * (int64_t)k + 1) = z.y;
     };
     if (c.pow2) {
       for (int ps = 0; ps < rs.n; ++ps) {
@@ -470,7 +498,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
     k_ring_analysis(RingParams p, int task0) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, task0 + blockIdx.x);
-  const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N, M = c.M;
+  const int lg = c.lg, n = c.n, N = c.N, M = c.M;
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
@@ -480,21 +508,25 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
   const Radices rs = radices(M);
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
-  for (int side = 0; side < 2; ++side) {
+  const int gmm = (1 << c.lgm) - 1;
+  for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;
-    const double *in = p.map_in + (side ? c.R.off_south : c.R.off_north) * p.nmaps + c.map0;
+    auto in_row = [&](int g, int64_t pix) -> const double * {
+      const int64_t off = lane_side(c, g, side) ? c.R.off_south : c.R.off_north;
+      return p.map_in + (off + pix) * p.nmaps + c.map0 + lane_map(c, g);
+    };
     auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, lg)]; };
     auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, lg)] = v; };
     // power of two: the DIT input position pos holds z[bitrev(pos)]
     auto pix_dit = [&](int pos, int g) -> cplx {
-      if (g >= c.nm) return {0.0, 0.0};
-      const int64_t s = bitrev((unsigned)pos, c.bits);
-      return {in[(2 * s) * p.nmaps + g], in[(2 * s + 1) * p.nmaps + g]};
+      if (!lane_live(c, g, side)) return {0.0, 0.0};
+      const int64_t s2 = 2 * (int64_t)bitrev((unsigned)pos, c.bits);
+      return {*in_row(g, s2), *in_row(g, s2 + 1)};
     };
     // Bluestein: chirped input z[k], zero beyond N
     auto pix_blue = [&](int k, int g) -> cplx {
-      if (k >= N || g >= c.nm) return {0.0, 0.0};
-      const cplx z = {in[(2 * (int64_t)k) * p.nmaps + g], in[(2 * (int64_t)k + 1) * p.nmaps + g]};
+      if (k >= N || !lane_live(c, g, side)) return {0.0, 0.0};
+      const cplx z = {*in_row(g, 2 * (int64_t)k), *in_row(g, 2 * (int64_t)k + 1)};
       return cmul(z, cconj(ring_chirp(p, c.R, k)));
     };
     auto zstore = [&](int k, int g, cplx v) {
@@ -521,11 +553,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
         }
       }
     }
-    // fold the spectrum F[k] (k <= N, from Z in natural order) into q~:
-    // g_m = F[m mod n] or its mirror
-    for (int t = threadIdx.x; t < ((p.mmax + 1) << lg); t += blockDim.x) {
-      const int g = t & gm, m = t >> lg;
-      if (g >= c.nm) continue;
+    // fold the spectrum F[k] (k <= N, from Z in natural order) of a lane into
+    // g_m = F[m mod n] or its mirror, times e^{-i m phi0} and the scale
+    auto fold = [&](int m, int g) -> cplx {
       const int jm = m % n;
       const bool mirror = jm > N;
       const int k = mirror ? n - jm : jm;
@@ -537,16 +567,28 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
       const cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
       cplx Fk = cadd(E, cmul(cconj(ring_root(p, c.R, k)), O));
       if (mirror) Fk = cconj(Fk);
-      const cplx gv = cscale(cmul(Fk, cconj(phase_at(plo, phi, m))), p.scale);
-      double *qe = qbase + m * qstride + 2 * g;
+      return cscale(cmul(Fk, cconj(phase_at(plo, phi, m))), p.scale);
+    };
+    for (int t = threadIdx.x; t < ((p.mmax + 1) << c.lgm); t += blockDim.x) {
+      const int mi = t & gmm, m = t >> c.lgm;
+      if (mi >= c.nm) continue;
+      double *qe = qbase + m * qstride + 2 * mi;
       double *qo = qe + half;
-      if (side == 0) {
-        *reinterpret_cast<double2 *>(qe) = make_double2(gv.x, gv.y);
-        *reinterpret_cast<double2 *>(qo) = make_double2(gv.x, gv.y);
+      if (c.two) {
+        // both hemispheres: q~_even = g_N + g_S, q~_odd = g_N - g_S (g_S = 0 at the equator)
+        const cplx gN = fold(m, mi), gS = fold(m, (1 << c.lgm) | mi);
+        *reinterpret_cast<double2 *>(qe) = make_double2(gN.x + gS.x, gN.y + gS.y);
+        *reinterpret_cast<double2 *>(qo) = make_double2(gN.x - gS.x, gN.y - gS.y);
       } else {
-        const cplx e = ld2(qe), o = ld2(qo);
-        *reinterpret_cast<double2 *>(qe) = make_double2(e.x + gv.x, e.y + gv.y);
-        *reinterpret_cast<double2 *>(qo) = make_double2(o.x - gv.x, o.y - gv.y);
+        const cplx gv = fold(m, mi);
+        if (side == 0) {
+          *reinterpret_cast<double2 *>(qe) = make_double2(gv.x, gv.y);
+          *reinterpret_cast<double2 *>(qo) = make_double2(gv.x, gv.y);
+        } else {
+          const cplx e = ld2(qe), o = ld2(qo);
+          *reinterpret_cast<double2 *>(qe) = make_double2(e.x + gv.x, e.y + gv.y);
+          *reinterpret_cast<double2 *>(qo) = make_double2(o.x - gv.x, o.y - gv.y);
+        }
       }
     }
     __syncthreads();
