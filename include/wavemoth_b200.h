@@ -131,6 +131,10 @@ void wavemoth_set_device_memory_cap(int64_t bytes);
    for the recorded events. */
 int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out);
 
+/* Number of this library's kernels launched by the plan's executes since the
+   last wavemoth_plan_timing reset (mode 0 or 1); -1 for a NULL plan. */
+int64_t wavemoth_plan_kernel_launches(wavemoth_plan plan);
+
 /* Algorithmic work of one transform direction of the plan for nmaps maps:
    out[0] Legendre flops (2 per multiply-add, 5 per recurrence step),
    out[1] compressed-matrix bytes read, out[2] alm + q bytes of one Legendre

@@ -101,13 +101,15 @@ struct _wavemoth_plan {
   wm::DevRingTask *d_ring_tasks = nullptr;
   double *d_twiddles = nullptr, *d_filters = nullptr, *d_ring_aux = nullptr;
   int32_t twlen = 0, max_bluestein = 0;
-  int32_t ring_ntasks0 = 0, ring_ntasks1 = 0, ring_smem0 = 0, ring_smem1 = 0, nphase_hi = 1;
+  int32_t ring_ntasks = 0, ring_smem = 0, nphase_hi = 1;
   double *d_alm = nullptr, *d_map = nullptr, *d_q = nullptr, *d_scratch = nullptr;
   int64_t slot_stride = 0;
   cudaStream_t stream = nullptr;
 
   // optional per-kernel event timing (wavemoth_plan_timing)
   bool timing = false;
+  // kernels launched by executes since the last timing reset
+  int64_t kernel_launches = 0;
   struct Span { int kind; cudaEvent_t a, b; };
   std::vector<Span> spans;
 
@@ -159,21 +161,21 @@ bool read_file(const std::string &path, std::vector<char> &buf, std::string &err
 
 struct RingTable {
   std::vector<wm::DevRing> rings;
-  std::vector<wm::DevRingTask> tasks;  // class 0, then class 1
+  std::vector<wm::DevRingTask> tasks;  // by decreasing cost
   int64_t filter_cplx = 0;   // complex entries of all Bluestein filter spectra
   int64_t aux_cplx = 0;      // complex entries of all Bluestein chirp/root tables
   int32_t twlen = 4;         // largest power-of-two table length needed
   int32_t max_bluestein = 0;
-  int32_t ntasks0 = 0, ntasks1 = 0;
-  int32_t smem0 = 0, smem1 = 0;
+  int32_t smem = 0;
   int32_t nphase_hi = 1;
   int64_t max_cta_cplx = 0;  // largest transform buffer of one CTA
 };
 
 // Ring geometry (src/wavemoth.c:1199-1232) and the CTA work list of the ring
-// kernels: per ring pair, groups of G maps with G x (transform length) within
-// the class-0 shared-memory budget; longer transforms run one map per CTA in
-// class 1.  Each class is ordered by decreasing cost.
+// kernels: per ring pair, groups of G maps with both hemispheres and
+// 2 G x (transform length) within the CTA buffer; transforms longer than half
+// the buffer run one map and one hemisphere per CTA.  Ordered by decreasing
+// cost so that the long transforms start first.
 RingTable ring_table(int nside, int nmaps, int mmax) {
   const int nrings = 4 * nside - 1, mid = 2 * nside - 1;
   std::vector<int64_t> offs(nrings + 1);
@@ -201,7 +203,7 @@ RingTable ring_table(int nside, int nmaps, int mmax) {
   T.nphase_hi = mmax / 64 + 1;
   int gmax = 1;
   while (gmax < nmaps && gmax < 8) gmax <<= 1;
-  struct Item { double cost; wm::DevRingTask t; int cls; int64_t cplx; };
+  struct Item { double cost; wm::DevRingTask t; int64_t cplx; };
   std::vector<Item> items;
   for (int r = 0; r < 2 * nside; ++r) {
     wm::DevRing R{};
@@ -227,34 +229,26 @@ RingTable ring_table(int nside, int nmaps, int mmax) {
       T.twlen = std::max(T.twlen, 2 * N);  // roots e^{2 pi i k / n}, n = 2N
     }
     T.rings[r] = R;
-    // both hemispheres in one CTA (lanes = sides x maps) when they fit a
-    // class; the longest transforms run one hemisphere at a time
-    int G = 1, cls = 1, two = 1;
-    if (2 * len <= wm::kRingBufferCplx) {
-      cls = 0;
-      G = std::min(gmax, wm::kRingBufferCplx / (2 * len));
-    } else if (2 * len > 2 * wm::kRingBufferCplx) {
-      two = 0;
-    }
+    // both hemispheres in one CTA (lanes = sides x maps) when they fit the
+    // buffer; the longest transforms run one hemisphere at a time
+    int G = 1, two = 1;
+    if (2 * len <= wm::kRingBufferCplx) G = std::min(gmax, wm::kRingBufferCplx / (2 * len));
+    else two = 0;
     int lg = 0;
     while ((1 << lg) < G) ++lg;
     const int64_t cplx = (int64_t)G * len << two;
     const double cost = (double)cplx * (R.bluestein_m ? 2.5 : 1.0) + (double)G * (mmax + 1);
     T.max_cta_cplx = std::max(T.max_cta_cplx, cplx);
     for (int g0 = 0; g0 < nmaps; g0 += G)
-      items.push_back({cost, wm::DevRingTask{r, g0, lg, two}, cls, cplx});
+      items.push_back({cost, wm::DevRingTask{r, g0, lg, two}, cplx});
   }
-  std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
-    return a.cls != b.cls ? a.cls < b.cls : a.cost > b.cost;
-  });
-  int64_t need[2] = {0, 0};
+  std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
+  int64_t need = 0;
   for (const Item &it : items) {
     T.tasks.push_back(it.t);
-    (it.cls ? T.ntasks1 : T.ntasks0)++;
-    need[it.cls] = std::max(need[it.cls], it.cplx);
+    need = std::max(need, it.cplx);
   }
-  T.smem0 = T.ntasks0 ? wm::ring_cta_smem(need[0], T.nphase_hi) : 0;
-  T.smem1 = T.ntasks1 ? wm::ring_cta_smem(need[1], T.nphase_hi) : 0;
+  T.smem = T.tasks.empty() ? 0 : wm::ring_cta_smem(need, T.nphase_hi);
   return T;
 }
 
@@ -420,14 +414,12 @@ wavemoth_plan make_plan(bool analysis, int Nside, int lmax, int mmax, int nmaps,
   rc = rc ? rc : A.alloc(&P->d_xbuf, (size_t)std::max<int64_t>(G.xrows, 1) * P->nvecs, "X buffer");
   {
     RingTable RT = ring_table(P->nside, nmaps, mmax);
-    if (!rc && RT.max_cta_cplx > 2 * wm::kRingBufferCplx)
+    if (!rc && RT.max_cta_cplx > wm::kRingBufferCplx)
       rc = set_error(WAVEMOTH_ERR_ARG, "ring transforms longer than 8192 points (nside > 2048) are not supported");
     P->twlen = RT.twlen;
     P->max_bluestein = RT.max_bluestein;
-    P->ring_ntasks0 = RT.ntasks0;
-    P->ring_ntasks1 = RT.ntasks1;
-    P->ring_smem0 = RT.smem0;
-    P->ring_smem1 = RT.smem1;
+    P->ring_ntasks = (int32_t)RT.tasks.size();
+    P->ring_smem = RT.smem;
     P->nphase_hi = RT.nphase_hi;
     rc = rc ? rc : upload(A, &P->d_rings, RT.rings, "ring table");
     rc = rc ? rc : upload(A, &P->d_ring_tasks, RT.tasks, "ring work list");
@@ -571,10 +563,8 @@ wm::RingParams ring_params(wavemoth_plan P) {
   r.aux = reinterpret_cast<const double2 *>(P->d_ring_aux);
   r.max_bluestein_m = P->max_bluestein;
   r.tasks = P->d_ring_tasks;
-  r.ntasks0 = P->ring_ntasks0;
-  r.ntasks1 = P->ring_ntasks1;
-  r.smem0 = P->ring_smem0;
-  r.smem1 = P->ring_smem1;
+  r.ntasks = P->ring_ntasks;
+  r.smem = P->ring_smem;
   r.nphase_hi = P->nphase_hi;
   return r;
 }
@@ -618,14 +608,20 @@ int run_split(wavemoth_plan P, bool alm2map, const double *alm_in, double *alm_o
     // alm2map: residual (alm -> X, q) then levels (X -> q); map2alm reversed
     auto residual = [&]() {
       rc = cuda_check(wm::launch_split(alm2map ? 0 : 2, s, gop, st), "operand slice launch");
-      if (!rc && nt)
+      P->kernel_launches++;
+      if (!rc && nt) {
         rc = cuda_check(wm::launch_split(alm2map ? 1 : 3, s, std::min(nt, P->sm_count), st), "split GEMM launch");
+        P->kernel_launches++;
+      }
     };
     auto levels = [&]() {
       if (!nl) return;
       rc = cuda_check(wm::launch_split(alm2map ? 4 : 6, s, gop_l, st), "level operand slice launch");
-      if (!rc)
+      P->kernel_launches++;
+      if (!rc) {
         rc = cuda_check(wm::launch_split(alm2map ? 5 : 7, s, std::min(nl, P->sm_count), st), "level GEMM launch");
+        P->kernel_launches++;
+      }
     };
     if (alm2map) {
       residual();
@@ -655,9 +651,11 @@ int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *al
   } else if (alm2map) {
     if (nta) rc = cuda_check(wm::launch_fast(0, f, fast_grid(P, nta), st), "alm2map residual launch");
     if (!rc && nr) rc = cuda_check(wm::launch_fast(1, f, fast_grid(P, nr), st), "alm2map level launch");
+    P->kernel_launches += (nta > 0) + (nr > 0);
   } else {
     if (nr) rc = cuda_check(wm::launch_fast(2, f, fast_grid(P, nr), st), "map2alm level launch");
     if (!rc && ntb) rc = cuda_check(wm::launch_fast(3, f, fast_grid(P, ntb), st), "map2alm residual launch");
+    P->kernel_launches += (ntb > 0) + (nr > 0);
   }
   if (!rc && P->nslow > 0) {
     wm::LegendreParams p = legendre_params(P);
@@ -671,6 +669,7 @@ int run_legendre(wavemoth_plan P, bool alm2map, const double *alm_in, double *al
     if (!rc)
       rc = cuda_check(wm::launch_legendre(alm2map, p, std::min(P->grid, std::max(1, (int)P->nslow)), st),
                       "Legendre kernel launch");
+    P->kernel_launches++;
   }
   span_end(P, sp, st);
   return rc;
@@ -683,6 +682,7 @@ int run_alm2map(wavemoth_plan P, const double *alm, double *map, cudaStream_t st
   r.map = map;
   int sp = span_begin(P, 2, st);
   int rc = cuda_check(wm::launch_ring_synthesis(r, st), "ring synthesis launch");
+  P->kernel_launches += r.ntasks > 0;
   span_end(P, sp, st);
   return rc;
 }
@@ -693,6 +693,7 @@ int run_map2alm(wavemoth_plan P, const double *map, double *alm, cudaStream_t st
   r.q_out = P->d_q;
   int sp = span_begin(P, 3, st);
   int rc0 = cuda_check(wm::launch_ring_analysis(r, st), "ring analysis launch");
+  P->kernel_launches += r.ntasks > 0;
   span_end(P, sp, st);
   if (rc0) return rc0;
   return run_legendre(P, false, nullptr, alm, P->d_q, nullptr, st);
@@ -856,6 +857,7 @@ void wavemoth_perform_backward_ffts(wavemoth_plan plan) {
     r.q = plan->d_q;
     r.map = devptr ? plan->host_out : plan->d_map;
     rc = cuda_check(wm::launch_ring_synthesis(r, plan->stream), "ring synthesis launch");
+    plan->kernel_launches += r.ntasks > 0;
     if (!rc && !devptr)
       rc = cuda_check(cudaMemcpyAsync(plan->host_out, plan->d_map,
                                       (size_t)plan->npix * plan->nmaps * sizeof(double),
@@ -894,6 +896,7 @@ int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out) {
     for (auto &s : plan->spans) { cudaEventDestroy(s.a); cudaEventDestroy(s.b); }
     plan->spans.clear();
     plan->timing = (mode == 1);
+    plan->kernel_launches = 0;
     return 0;
   }
   if (mode != 2 || !out) return set_error(WAVEMOTH_ERR_ARG, "invalid timing mode");
@@ -907,6 +910,8 @@ int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out) {
   }
   return 0;
 }
+
+int64_t wavemoth_plan_kernel_launches(wavemoth_plan plan) { return plan ? plan->kernel_launches : -1; }
 
 int wavemoth_plan_work(wavemoth_plan plan, int nmaps, double *out) {
   if (!plan || !out || nmaps <= 0) return set_error(WAVEMOTH_ERR_ARG, "invalid arguments");

@@ -128,11 +128,11 @@ struct RingParams {
   const double2 *aux;     // Bluestein chirps and roots of unity per ring
   double *aux_out;        // written at plan creation
   int32_t max_bluestein_m;
-  // CTA work list: class 0 (tasks [0, ntasks0)) then class 1, each launched
-  // with its own dynamic shared memory size
+  // CTA work list (one CTA per task, ordered by decreasing cost) and the
+  // dynamic shared memory of every CTA
   const DevRingTask *tasks;
-  int32_t ntasks0, ntasks1;
-  int32_t smem0, smem1;   // bytes
+  int32_t ntasks;
+  int32_t smem;           // bytes
   int32_t nphase_hi;      // entries of the coarse phase table (mmax / 64 + 1)
 };
 
@@ -143,6 +143,6 @@ cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *f
 // Shared-memory bytes of a ring CTA whose transform buffer holds `cplx`
 // complex values per map lane times the lanes.
 int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi);
-constexpr int32_t kRingBufferCplx = 4096;  // class-0 budget: 64 KB of transform buffer
+constexpr int32_t kRingBufferCplx = 8192;  // transform buffer of one CTA: 128 KB
 
 }  // namespace wm

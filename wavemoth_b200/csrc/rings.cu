@@ -30,24 +30,27 @@
 //     in the DIF output order) and DIT back; the last DIF pass, the product
 //     and the first DIT pass share one register pass.
 // Within a radix-16 pass the twiddles of radix-2 stage s at offset
-// j + m (len / 16) factor as w_{len / 2^s}^j (one table lookup per stage)
-// times a 16th root of unity fixed at compile time.  Twiddles come from one
-// table of e^{2 pi i k / TW}, TW the largest power of two used; chirps
-// e^{i pi k^2 / N} and roots e^{2 pi i k / n} of the Bluestein rings from a
-// per-ring table; all computed at plan creation with sincospi on exact
-// rationals.
+// j + m (len / 16) factor as w_{len / 2^s}^j (one table lookup per stage,
+// all four issued before the butterfly's points are loaded; every length is
+// a power of two, so the index is a shift of j) times a 16th root of unity
+// fixed at compile time.  Twiddles come from one table of e^{2 pi i k / TW},
+// TW the largest power of two used; chirps e^{i pi k^2 / N} and roots
+// e^{2 pi i k / n} of the Bluestein rings from a per-ring table; all computed
+// at plan creation with sincospi on exact rationals.
 //
-// Work decomposition: one CTA per (ring pair, group of G = 2^lg maps), G
-// chosen per ring so that the transform buffer (G x N or G x M complex) fits
-// 64 KB (4096 complex: 16 points per thread at 256 threads); longer
-// transforms run one map per CTA of 512 threads.  The G maps are the fastest
-// index of the thread layout: lanes g = 0..G-1 of a warp handle the same
-// bin, pixel or butterfly of G maps, so q rows and map pixels are read and
-// written as G-map runs and twiddles, chirps and phases are shared.
-// In shared memory element i of map lane g is at slot(i) * G + g with the XOR
+// Work decomposition: one CTA of 512 threads per (ring pair, group of G = 2^lg
+// maps) with a 128 KB transform buffer (8192 complex, 16 points per thread).
+// Both hemispheres of the pair share the CTA when 2 G x N (or 2 G x M) fits
+// the buffer: lanes are (side, map), so synthesis reads every q element once
+// and analysis writes every q~ element once; longer transforms (nside 2048)
+// run one hemisphere at a time.  Lanes are the fastest index of the thread
+// layout: lanes of a warp handle the same bin, pixel or butterfly of
+// different maps, so q rows and map pixels are read and written as G-map runs
+// and twiddles, chirps and phases are shared.
+// In shared memory element i of lane g is at slot(i) * lanes + g with the XOR
 // swizzle slot(i) = i ^ ((i >> 4) & 15), a permutation inside each aligned
 // group of 16 that makes the 16-byte accesses of every pass of radix 2..16
-// conflict-free for G = 1, 2, 4, 8.
+// conflict-free for 1, 2, 4, 8 and 16 lanes.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -59,8 +62,7 @@ namespace wm {
 namespace {
 
 constexpr int kRadixLog = 4;           // largest pass radix 2^kRadixLog
-constexpr int kRingThreads = 256;      // class 0: <= 4096 complex per CTA
-constexpr int kRingThreadsWide = 512;  // class 1: <= 8192 complex per CTA
+constexpr int kRingThreads = 512;      // 16 points per thread of a kRingBufferCplx buffer
 constexpr int kPhaseLo = 64;           // e^{i m phi0} = hi[m / 64] * lo[m % 64]
 
 struct cplx {
@@ -129,36 +131,48 @@ template <> struct Log2<4> { static constexpr int v = 2; };
 template <> struct Log2<8> { static constexpr int v = 3; };
 template <> struct Log2<16> { static constexpr int v = 4; };
 
-// Radix-R decimation-in-frequency butterfly of the points j + i (len / R),
-// i < R, of one block of length len: log2 R radix-2 stages in registers.
+// Stage twiddles of a radix-R butterfly at offset j of a block of length
+// 2^lglen, fetched before the butterfly's points: DIF stage s uses
+// w_{len / 2^s}^j, DIT stage s uses w_{2^(s+1) len / R}^j.  All lengths are
+// powers of two, so the table index is a shift of j.
+template <int R, int SIGN, bool DIF>
+__device__ __forceinline__ void stage_twiddles(cplx (&A)[Log2<R>::v], int j, int lglen, const double2 *tw,
+                                               int lgtw) {
+#pragma unroll
+  for (int s = 0; s < Log2<R>::v; ++s) {
+    const int sh = DIF ? lgtw - lglen + s : lgtw - lglen + Log2<R>::v - (s + 1);
+    A[s] = twiddle<SIGN>(tw, j << sh);
+  }
+}
+
+// Radix-R decimation-in-frequency butterfly of R points in registers:
+// log2 R radix-2 stages, stage s multiplied by A[s] and a 16th root.
 template <int R, int SIGN>
-__device__ __forceinline__ void dif_regs(cplx (&x)[R], int j, int len, const double2 *tw, int twlen) {
+__device__ __forceinline__ void dif_regs(cplx (&x)[R], const cplx (&A)[Log2<R>::v]) {
 #pragma unroll
   for (int s = 0; s < Log2<R>::v; ++s) {
     const int h = R >> (s + 1);
-    const cplx A = twiddle<SIGN>(tw, j * (twlen / (len >> s)));  // w_{len / 2^s}^j
 #pragma unroll
     for (int i = 0; i < R / 2; ++i) {
       const int lo = (i / h) * 2 * h + (i % h), hi = lo + h, m = i % h;
       const cplx u = x[lo], v = x[hi];
       x[lo] = cadd(u, v);
-      x[hi] = mul_root16<SIGN>(cmul(csub(u, v), A), (m << s) * (16 / R));
+      x[hi] = mul_root16<SIGN>(cmul(csub(u, v), A[s]), (m << s) * (16 / R));
     }
   }
 }
 
-// Radix-R decimation-in-time butterfly of the points j + i (len / R).
+// Radix-R decimation-in-time butterfly of R points in registers.
 template <int R, int SIGN>
-__device__ __forceinline__ void dit_regs(cplx (&x)[R], int j, int len, const double2 *tw, int twlen) {
+__device__ __forceinline__ void dit_regs(cplx (&x)[R], const cplx (&A)[Log2<R>::v]) {
 #pragma unroll
   for (int s = 0; s < Log2<R>::v; ++s) {
     const int h = 1 << s;
-    const cplx A = twiddle<SIGN>(tw, j * (twlen / ((len / R) << (s + 1))));  // w_L^j
 #pragma unroll
     for (int i = 0; i < R / 2; ++i) {
       const int lo = (i / h) * 2 * h + (i % h), hi = lo + h, m = i % h;
       const cplx u = x[lo];
-      const cplx t = mul_root16<SIGN>(cmul(x[hi], A), m << (4 - (s + 1)));
+      const cplx t = mul_root16<SIGN>(cmul(x[hi], A[s]), m << (4 - (s + 1)));
       x[lo] = cadd(u, t);
       x[hi] = csub(u, t);
     }
@@ -171,73 +185,87 @@ __device__ __forceinline__ void dit_regs(cplx (&x)[R], int j, int len, const dou
 namespace wm {
 namespace {
 
+// Shared arguments of the passes of one CTA: the twiddle table (2^lgtw
+// entries), the transform length M and the log2 of the lanes.
+struct FftCtx {
+  const double2 *tw;
+  int lgtw;
+  int M;
+  int lg;
+};
+
 // One in-place pass of radix R over the 2^lg interleaved sequences of length
-// M: butterfly b of lane g takes the points base + i q (q = len / R) of its
-// block, through `load(index, g)` and `store(index, g, value)`.
+// M: butterfly b of lane g takes the points base + i q (q = len / R, len =
+// 2^lglen) of its block, through `load(index, g)` and `store(index, g, value)`.
 template <int R, int SIGN, bool DIF, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_pass(int M, int len, int lg, const double2 *tw, int twlen, LoadF load,
-                                         StoreF store) {
-  const int gm = (1 << lg) - 1, q = len / R, lq = ilog2(q);
-  const int nbf = (M / R) << lg;
+__device__ __forceinline__ void fft_pass(const FftCtx &f, int lglen, LoadF load, StoreF store) {
+  constexpr int LR = Log2<R>::v;
+  const int gm = (1 << f.lg) - 1, lq = lglen - LR;
+  const int nbf = (f.M >> LR) << f.lg;
   for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
-    const int g = t & gm, b = t >> lg;
-    const int j = b & (q - 1), base = (b >> lq) * len + j;
+    const int g = t & gm, b = t >> f.lg;
+    const int j = b & ((1 << lq) - 1), base = ((b >> lq) << lglen) + j;
+    cplx A[LR];
+    stage_twiddles<R, SIGN, DIF>(A, j, lglen, f.tw, f.lgtw);
     cplx x[R];
 #pragma unroll
-    for (int i = 0; i < R; ++i) x[i] = load(base + i * q, g);
-    if (DIF) dif_regs<R, SIGN>(x, j, len, tw, twlen);
-    else dit_regs<R, SIGN>(x, j, len, tw, twlen);
+    for (int i = 0; i < R; ++i) x[i] = load(base + (i << lq), g);
+    if (DIF) dif_regs<R, SIGN>(x, A);
+    else dit_regs<R, SIGN>(x, A);
 #pragma unroll
-    for (int i = 0; i < R; ++i) store(base + i * q, g, x[i]);
+    for (int i = 0; i < R; ++i) store(base + (i << lq), g, x[i]);
   }
   __syncthreads();
 }
 
 template <int SIGN, bool DIF, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_pass_r(int R, int M, int len, int lg, const double2 *tw, int twlen,
-                                           LoadF load, StoreF store) {
+__device__ __forceinline__ void fft_pass_r(const FftCtx &f, int R, int lglen, LoadF load, StoreF store) {
   switch (R) {
-    case 2: fft_pass<2, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
-    case 4: fft_pass<4, SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    case 2: fft_pass<2, SIGN, DIF>(f, lglen, load, store); break;
+    case 4: fft_pass<4, SIGN, DIF>(f, lglen, load, store); break;
     case 8:
       if (kRadixLog > 3) {
-        fft_pass<8, SIGN, DIF>(M, len, lg, tw, twlen, load, store);
+        fft_pass<8, SIGN, DIF>(f, lglen, load, store);
         break;
       }
       [[fallthrough]];
-    default: fft_pass<(1 << kRadixLog), SIGN, DIF>(M, len, lg, tw, twlen, load, store); break;
+    default: fft_pass<(1 << kRadixLog), SIGN, DIF>(f, lglen, load, store); break;
   }
 }
 
 // Middle of Bluestein's convolution on blocks of R points (R = the last DIF
 // radix = the first DIT radix): forward DIF stages, the product with the
 // filter spectrum (stored in DIF output order; the sign -1 filter is its
-// reflection F'(k) = conj F(-k)), inverse DIT stages.
+// reflection F'(k) = conj F(-k)), inverse DIT stages.  Block offset 0: every
+// stage twiddle is 1.
 template <int R, class LoadF, class StoreF>
-__device__ __forceinline__ void bluestein_mid_r(int M, int lg, const cplx *F, int fsign, const double2 *tw,
-                                                int twlen, LoadF load, StoreF store) {
-  const int gm = (1 << lg) - 1, bitsM = ilog2(M);
-  const int nbf = (M / R) << lg;
+__device__ __forceinline__ void bluestein_mid_r(const FftCtx &f, const cplx *F, int fsign, LoadF load,
+                                                StoreF store) {
+  const int gm = (1 << f.lg) - 1, bitsM = ilog2(f.M);
+  const int nbf = (f.M / R) << f.lg;
+  cplx one[Log2<R>::v];
+#pragma unroll
+  for (int s = 0; s < Log2<R>::v; ++s) one[s] = {1.0, 0.0};
   for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
-    const int g = t & gm, base = (t >> lg) * R;
+    const int g = t & gm, base = (t >> f.lg) * R;
     cplx x[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) x[i] = load(base + i, g);
-    dif_regs<R, -1>(x, 0, R, tw, twlen);
+    dif_regs<R, -1>(x, one);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int k = base + i;
-      cplx f;
+      cplx fk;
       if (fsign > 0) {
-        f = F[k];
+        fk = F[k];
       } else {
         const unsigned natural = bitrev((unsigned)k, bitsM);
-        const unsigned refl = (M - natural) & (M - 1);
-        f = cconj(F[bitrev(refl, bitsM)]);
+        const unsigned refl = (f.M - natural) & (f.M - 1);
+        fk = cconj(F[bitrev(refl, bitsM)]);
       }
-      x[i] = cmul(x[i], f);
+      x[i] = cmul(x[i], fk);
     }
-    dit_regs<R, 1>(x, 0, R, tw, twlen);
+    dit_regs<R, 1>(x, one);
 #pragma unroll
     for (int i = 0; i < R; ++i) store(base + i, g, x[i]);
   }
@@ -245,44 +273,39 @@ __device__ __forceinline__ void bluestein_mid_r(int M, int lg, const cplx *F, in
 }
 
 template <class LoadF, class StoreF>
-__device__ __forceinline__ void bluestein_mid(int R, int M, int lg, const cplx *F, int fsign, const double2 *tw,
-                                              int twlen, LoadF load, StoreF store) {
+__device__ __forceinline__ void bluestein_mid(const FftCtx &f, int R, const cplx *F, int fsign, LoadF load,
+                                              StoreF store) {
   switch (R) {
-    case 2: bluestein_mid_r<2>(M, lg, F, fsign, tw, twlen, load, store); break;
-    case 4: bluestein_mid_r<4>(M, lg, F, fsign, tw, twlen, load, store); break;
+    case 2: bluestein_mid_r<2>(f, F, fsign, load, store); break;
+    case 4: bluestein_mid_r<4>(f, F, fsign, load, store); break;
     case 8:
       if (kRadixLog > 3) {
-        bluestein_mid_r<8>(M, lg, F, fsign, tw, twlen, load, store);
+        bluestein_mid_r<8>(f, F, fsign, load, store);
         break;
       }
       [[fallthrough]];
-    default: bluestein_mid_r<(1 << kRadixLog)>(M, lg, F, fsign, tw, twlen, load, store); break;
+    default: bluestein_mid_r<(1 << kRadixLog)>(f, F, fsign, load, store); break;
   }
 }
 
 // Pass radices of a length-M transform in DIF order: 2^(log2 M mod 4) (if
-// above 1) then 16s.  DIT runs them in reverse order.
+// above 1) then 16s.  DIT runs them in reverse order.  Computed per pass
+// (no per-thread arrays, which would live in local memory).
 struct Radices {
-  int n;         // number of passes
-  int r[8];      // radix of DIF pass p
-  int len[8];    // block length of DIF pass p (the DIT pass mirroring it has the same)
+  int lgM;  // log2 M
+  int r0;   // log2 M mod 4: log2 of the radix of the first DIF pass, 0 if none
+  int n;    // number of passes
+  // radix of DIF pass p
+  __device__ __forceinline__ int r(int p) const { return (p == 0 && r0) ? 1 << r0 : 1 << kRadixLog; }
+  // log2 of the block length of DIF pass p (the DIT pass mirroring it has the same)
+  __device__ __forceinline__ int lgl(int p) const { return p == 0 ? lgM : lgM - r0 - kRadixLog * (p - (r0 ? 1 : 0)); }
 };
 
 __device__ __forceinline__ Radices radices(int M) {
   Radices s;
-  const int lgM = ilog2(M), r0 = lgM % kRadixLog;
-  s.n = 0;
-  int len = M;
-  if (r0) {
-    s.r[s.n] = 1 << r0;
-    s.len[s.n++] = len;
-    len >>= r0;
-  }
-  for (int k = 0; k < lgM / kRadixLog; ++k) {
-    s.r[s.n] = 1 << kRadixLog;
-    s.len[s.n++] = len;
-    len >>= kRadixLog;
-  }
+  s.lgM = ilog2(M);
+  s.r0 = s.lgM % kRadixLog;
+  s.n = s.lgM / kRadixLog + (s.r0 ? 1 : 0);
   return s;
 }
 
@@ -305,7 +328,7 @@ __device__ __forceinline__ cplx ring_root(const RingParams &p, const DevRing &R,
   const int N = R.n >> 1;
   if (R.bluestein_m == 0) {
     if (k == N) return {-1.0, 0.0};
-    const double2 t = p.twiddles[(int64_t)k * (p.twlen / R.n)];
+    const double2 t = p.twiddles[k << (ilog2(p.twlen) - ilog2(R.n))];
     return {t.x, t.y};
   }
   const double2 t = p.aux[R.aux + N + k];
@@ -395,11 +418,9 @@ __device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int m
   }
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog == 4 ? 2 : 3) : 1)
-    k_ring_synthesis(RingParams p, int task0) {
+__global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p) {
   extern __shared__ double smem_d[];
-  const RingCta c = ring_cta(p, task0 + blockIdx.x);
+  const RingCta c = ring_cta(p, blockIdx.x);
   const int lg = c.lg, gm = (1 << lg) - 1, n = c.n, N = c.N, M = c.M;
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   cplx *plo = buf + ((int64_t)M << lg);
@@ -409,6 +430,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   const double *qbase = p.q + (int64_t)c.ring * p.nvecs + 2 * c.map0;
   const Radices rs = radices(M);
+  const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   const int gmm = (1 << c.lgm) - 1;
@@ -473,31 +495,29 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
     };
     if (c.pow2) {
       for (int ps = 0; ps < rs.n; ++ps) {
-        if (ps == rs.n - 1) fft_pass_r<1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, pix_dif);
-        else fft_pass_r<1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+        if (ps == rs.n - 1) fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), sload, pix_dif);
+        else fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
       }
     } else {
       for (int ps = 0; ps < rs.n - 1; ++ps)
-        fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
-      const int R = rs.r[rs.n - 1];
+        fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+      const int R = rs.r(rs.n - 1);
       if (rs.n == 1) {
-        bluestein_mid(R, M, lg, F, +1, p.twiddles, p.twlen, sload, pix_blue);
+        bluestein_mid(fx, R, F, +1, sload, pix_blue);
       } else {
-        bluestein_mid(R, M, lg, F, +1, p.twiddles, p.twlen, sload, sstore);
+        bluestein_mid(fx, R, F, +1, sload, sstore);
         for (int ps = rs.n - 2; ps >= 0; --ps) {
-          if (ps == 0) fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, pix_blue);
-          else fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, pix_blue);
+          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
         }
       }
     }
   }
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog == 4 ? 2 : 3) : 1)
-    k_ring_analysis(RingParams p, int task0) {
+__global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p) {
   extern __shared__ double smem_d[];
-  const RingCta c = ring_cta(p, task0 + blockIdx.x);
+  const RingCta c = ring_cta(p, blockIdx.x);
   const int lg = c.lg, n = c.n, N = c.N, M = c.M;
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   cplx *plo = buf + ((int64_t)M << lg);
@@ -506,6 +526,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   double *qbase = p.q_out + (int64_t)c.ring * p.nvecs + 2 * c.map0;
   const Radices rs = radices(M);
+  const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   const int gmm = (1 << c.lgm) - 1;
@@ -534,22 +555,22 @@ __global__ void __launch_bounds__(THREADS, THREADS == kRingThreads ? (kRadixLog 
     };
     if (c.pow2) {
       for (int ps = rs.n - 1; ps >= 0; --ps) {
-        if (ps == rs.n - 1) fft_pass_r<-1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, pix_dit, sstore);
-        else fft_pass_r<-1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+        if (ps == rs.n - 1) fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), pix_dit, sstore);
+        else fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
       }
     } else {
       for (int ps = 0; ps < rs.n - 1; ++ps) {
-        if (ps == 0) fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, pix_blue, sstore);
-        else fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+        if (ps == 0) fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), pix_blue, sstore);
+        else fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
       }
-      const int R = rs.r[rs.n - 1];
+      const int R = rs.r(rs.n - 1);
       if (rs.n == 1) {
-        bluestein_mid(R, M, lg, F, -1, p.twiddles, p.twlen, pix_blue, zstore);
+        bluestein_mid(fx, R, F, -1, pix_blue, zstore);
       } else {
-        bluestein_mid(R, M, lg, F, -1, p.twiddles, p.twlen, sload, sstore);
+        bluestein_mid(fx, R, F, -1, sload, sstore);
         for (int ps = rs.n - 2; ps >= 0; --ps) {
-          if (ps == 0) fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, zstore);
-          else fft_pass_r<1, false>(rs.r[ps], M, rs.len[ps], lg, p.twiddles, p.twlen, sload, sstore);
+          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, zstore);
+          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
         }
       }
     }
@@ -618,7 +639,7 @@ __global__ void k_ring_aux(RingParams p) {
   }
 }
 
-__global__ void __launch_bounds__(kRingThreadsWide) k_bluestein_filters(RingParams p) {
+__global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p) {
   extern __shared__ double smem_d[];
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   const DevRing R = p.rings[blockIdx.x];
@@ -635,28 +656,20 @@ __global__ void __launch_bounds__(kRingThreadsWide) k_bluestein_filters(RingPara
   auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, 0)]; };
   auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, 0)] = v; };
   const Radices rs = radices(M);
+  const FftCtx fx{p.twiddles, ilog2(p.twlen), M, 0};
   for (int ps = 0; ps < rs.n; ++ps)
-    fft_pass_r<-1, true>(rs.r[ps], M, rs.len[ps], 0, p.twiddles, p.twlen, sload, sstore);
+    fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
   cplx *F = reinterpret_cast<cplx *>(p.filters_out) + R.filter;
   for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[at(k, 0, 0)];
 }
 
-template <class K0, class K1>
-cudaError_t launch_classes(K0 kernel0, K1 kernel1, const RingParams &prm, cudaStream_t st) {
-  cudaError_t e;
-  if (prm.ntasks0 > 0) {
-    e = cudaFuncSetAttribute(kernel0, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.smem0);
-    if (e != cudaSuccess) return e;
-    kernel0<<<prm.ntasks0, kRingThreads, prm.smem0, st>>>(prm, 0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  if (prm.ntasks1 > 0) {
-    e = cudaFuncSetAttribute(kernel1, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.smem1);
-    if (e != cudaSuccess) return e;
-    kernel1<<<prm.ntasks1, kRingThreadsWide, prm.smem1, st>>>(prm, prm.ntasks0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+template <class K>
+cudaError_t launch_rings(K kernel, const RingParams &prm, cudaStream_t st) {
+  if (prm.ntasks <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<prm.ntasks, kRingThreads, prm.smem, st>>>(prm);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -666,11 +679,11 @@ int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi) {
 }
 
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
-  return launch_classes(k_ring_synthesis<kRingThreads>, k_ring_synthesis<kRingThreadsWide>, prm, st);
+  return launch_rings(k_ring_synthesis, prm, st);
 }
 
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
-  return launch_classes(k_ring_analysis<kRingThreads>, k_ring_analysis<kRingThreadsWide>, prm, st);
+  return launch_rings(k_ring_analysis, prm, st);
 }
 
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters, double *aux,
@@ -687,7 +700,7 @@ cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *f
   const int smem = prm.max_bluestein_m * 2 * (int)sizeof(double);
   e = cudaFuncSetAttribute(k_bluestein_filters, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_bluestein_filters<<<prm.ni, kRingThreadsWide, smem, st>>>(q);
+  k_bluestein_filters<<<prm.ni, kRingThreads, smem, st>>>(q);
   return cudaGetLastError();
 }
 

@@ -95,7 +95,8 @@ class Transform:
         if mode != 2:
             return None
         keys = ("legendre_alm2map", "legendre_map2alm", "ring_synthesis", "ring_analysis")
-        return {"ms": dict(zip(keys, list(out)[:4])), "launches": dict(zip(keys, list(out)[4:]))}
+        return {"ms": dict(zip(keys, list(out)[:4])), "launches": dict(zip(keys, list(out)[4:])),
+                "kernels": int(_native.lib().wavemoth_plan_kernel_launches(self._plan))}
 
     def work(self):
         """Algorithmic work of one direction (see wavemoth_plan_work)."""
