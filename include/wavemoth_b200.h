@@ -22,6 +22,12 @@ extern "C" {
 #define WAVEMOTH_PRECISION_SPLIT 0x200   /* residual products of depth-0/1 matrices as sliced int8
                                             tensor-core GEMMs re-summed in FP64 (Ozaki scheme);
                                             the recurrence, seeds and scales stay FP64 */
+#define WAVEMOTH_SPLIT_GENERATE 0x400    /* with WAVEMOTH_PRECISION_SPLIT: generate the residual P
+                                            inside the GEMM kernels at every call instead of
+                                            slicing it once per plan into device memory (6 bytes
+                                            per element of the residual tiles, about 20 GB at
+                                            nside 1024); the plan also falls back to this when
+                                            the device lacks the memory.  Same results. */
 
 /* status codes */
 #define WAVEMOTH_OK 0

@@ -97,6 +97,25 @@ struct SplitParams {
   double2 *level_rs;              // row scales of W
 };
 
+// One launch of the streamed split GEMM: tiles whose A chunks were sliced
+// once per plan (residual P or level W) and whose B planes come from the
+// operand pre-pass of the call.
+struct StreamLaunch {
+  const DevStreamTile *tiles;
+  const int32_t *rows;    // ntiles x kSplitM destination rows (-1: none)
+  const int32_t *sidx;    // ntiles x kSplitM entries of `scales` (-1: none)
+  const double2 *scales;  // (2^e, 2^-e) of the P column / P row / W row of each tile row
+  const int8_t *a;        // A chunk pool
+  int32_t ntiles;
+  int32_t a_mn;           // 1: A chunks MN-major (map2alm residual), 0: K-major
+};
+cudaError_t launch_stream(const SplitParams &prm, const StreamLaunch &L, int grid, cudaStream_t st);
+// Plan creation: residual P of every alm2map tile (SplitParams::tiles_a
+// order, K-major chunks) and map2alm tile (tiles_b order, MN-major chunks)
+// sliced into the A pools of the two launches.
+cudaError_t launch_residual_slices(const SplitParams &prm, const StreamLaunch &a2m, const StreamLaunch &m2a,
+                                   cudaStream_t st);
+
 // which: 0 alm operand slices, 1 alm2map residual, 2 X operand slices, 3 map2alm residual,
 //        4 alm2map level operand (X) slices, 5 alm2map level GEMM,
 //        6 map2alm level operand (q~) slices, 7 map2alm level GEMM

@@ -397,16 +397,12 @@ __device__ __forceinline__ void issue_step(uint32_t tmem, uint32_t a_base, uint3
 }
 
 // FP64 value of the diagonal accumulators of one (lane, vector):
-// sum_k D_k 2^(70 - 7k).
+// 2^28 sum_k D_k 2^(42 - 7k), with the first and the second three diagonals
+// combined exactly in 64-bit integers (|D_k| < 2^31), then two roundings.
 __device__ __forceinline__ double recombine(const int32_t (&d)[kSplitDiag][8], int j) {
-  double s = (double)d[6][j];
-  s = fma((double)d[5][j], 0x1p7, s);
-  s = fma((double)d[4][j], 0x1p14, s);
-  s = fma((double)d[3][j], 0x1p21, s);
-  s = fma((double)d[2][j], 0x1p28, s);
-  s = fma((double)d[1][j], 0x1p35, s);
-  s = fma((double)d[0][j], 0x1p42, s);
-  return s * 0x1p28;
+  const long long hi = ((long long)d[0][j] << 14) + ((long long)d[1][j] << 7) + d[2][j];
+  const long long mid = ((long long)d[3][j] << 14) + ((long long)d[4][j] << 7) + d[5][j];
+  return fma((double)hi, 0x1p28, fma((double)mid, 0x1p7, (double)d[6][j])) * 0x1p28;
 }
 
 // P at rows r0 .. r0 + 15 of group column c (zero outside [C.start, nrows)):
@@ -983,7 +979,296 @@ __global__ void __launch_bounds__(kLevelThr, 1) k_level_split(SplitParams p) {
   if (warp == 0) tmem_free(tmem);
 }
 
+
+// ------------------------------------------------------------------------
+// Streamed split GEMM.  Both operands arrive pre-sliced from global memory
+// (A chunks cut once per plan, B planes by the operand pre-pass), so one
+// kernel serves the residual and level products of both directions.
+// Warp roles (one CTA per SM, persistent over the tile list):
+//   warp 0   one thread loads chunk after chunk with 1D bulk copies (TMA,
+//            no multicast) into kStreamStages stages, running ahead into the
+//            next tile while the current one drains;
+//   warp 1   one thread issues the nine MMAs per K step of 32 and commits
+//            each stage back to the loader, the finished tile to the
+//            epilogue;
+//   warps 2..9 drain TMEM (warp w reads lane quarter w % 4, vector half
+//            (w - 2) / 4), release it to the MMA thread, scale the FP64 tile
+//            into shared memory and write its rows to global memory while
+//            the next tile's MMAs run.
+// Every wait is bounded and also gives up when another role has recorded an
+// abort; the MMA thread then waits (bounded) for its MMAs and the loader for
+// its copies before the CTA frees TMEM and returns.
+// ------------------------------------------------------------------------
+constexpr int kStreamStages = 2;
+constexpr int kStreamEpiWarps = 8;
+constexpr int kStreamThr = 32 * (2 + kStreamEpiWarps);
+constexpr int kStreamStage = kStageA + kStageB;  // 73728 bytes
+
+struct StreamSmem {
+  uint64_t full[kStreamStages], empty[kStreamStages];
+  uint64_t acc_full, acc_empty, fin;
+  uint32_t tmem;
+  int32_t abort;
+};
+
+// Bounded wait that also ends when *abort is set; false unless completed.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t phase, volatile int32_t *abort) {
+  uint32_t done = 0;
+  for (long long it = 0; it < kWaitLimit; ++it) {
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase));
+    if (done) return true;
+    if ((it & 255) == 255 && *abort) return false;
+  }
+  *abort = 1;
+  return false;
+}
+
+// Barrier 1 over the epilogue warps with an OR of `v` (the same answer in
+// every epilogue thread, so they leave their loop together).
+__device__ __forceinline__ bool epi_sync_or(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(32 * kStreamEpiWarps)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 7 x 8 TMEM columns (the diagonals of 8 vectors) of this thread's lane with
+// one wait.
+__device__ __forceinline__ void tmem_ld_diags(uint32_t taddr, int32_t (&d)[kSplitDiag][8]) {
+#pragma unroll
+  for (int k = 0; k < kSplitDiag; ++k) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7])
+                 : "r"(taddr + 64 * k));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) d[k][j] = (int32_t)r[j];
+  }
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int kAmn>
+__global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, StreamLaunch L) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  StreamSmem *ss = reinterpret_cast<StreamSmem *>(smem + kStreamStages * kStreamStage);
+  double *xs = reinterpret_cast<double *>(smem + kStreamStages * kStreamStage + 128);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  volatile int32_t *abort = &ss->abort;
+  if (warp == 0) tmem_alloc(&ss->tmem);
+  if (tid == 0) {
+    for (int s = 0; s < kStreamStages; ++s) {
+      mbar_init(&ss->full[s], 1);
+      mbar_init(&ss->empty[s], 1);
+    }
+    mbar_init(&ss->acc_full, 1);
+    mbar_init(&ss->acc_empty, kStreamEpiWarps);
+    mbar_init(&ss->fin, 1);
+    ss->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = ss->tmem;
+  if (warp == 0) {
+    // ---------------- loader ----------------
+    if (lane == 0) {
+      long long g = 0;  // chunks issued
+      for (int t = blockIdx.x; t < L.ntiles && !*abort; t += gridDim.x) {
+        const DevStreamTile T = L.tiles[t];
+        for (int c = 0; c < T.nk; ++c, ++g) {
+          const int s = (int)(g % kStreamStages);
+          const long long use = g / kStreamStages;
+          if (use > 0 && !mbar_wait_or_abort(&ss->empty[s], (uint32_t)((use - 1) & 1), abort)) break;
+          const uint32_t dst = smem_u32(smem + s * kStreamStage);
+          expect_tx(&ss->full[s], kStreamStage);
+          bulk_load(dst, L.a + (T.a + c) * (int64_t)kStageA, kStageA, &ss->full[s]);
+          bulk_load(dst + kStageA, p.planes + (T.b + c) * (int64_t)kSplitPlane, kStageB, &ss->full[s]);
+        }
+      }
+      // every issued copy lands before the CTA may exit
+      for (int s = 0; s < kStreamStages; ++s) {
+        const long long n = g > s ? (g - 1 - s) / kStreamStages + 1 : 0;  // copies into stage s
+        if (n > 0) mbar_wait(&ss->full[s], (uint32_t)((n - 1) & 1));
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issue ----------------
+    if (lane == 0) {
+      long long g = 0;
+      int nt = 0;
+      for (int t = blockIdx.x; t < L.ntiles && !*abort; t += gridDim.x, ++nt) {
+        const DevStreamTile T = L.tiles[t];
+        if (nt > 0 && !mbar_wait_or_abort(&ss->acc_empty, (uint32_t)((nt - 1) & 1), abort)) break;
+        fence_after_sync();
+        bool ok = true;
+        for (int c = 0; c < T.nk; ++c, ++g) {
+          const int s = (int)(g % kStreamStages);
+          if (!mbar_wait_or_abort(&ss->full[s], (uint32_t)((g / kStreamStages) & 1), abort)) {
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          const uint32_t a0 = smem_u32(smem + s * kStreamStage), b0 = a0 + kStageA;
+          for (int ks = 0; ks < kSplitK / 32; ++ks) {
+            if (kAmn) issue_step(tmem, a0 + ks * 512, b0 + ks * 256, 1, 128, 1024, c == 0 && ks == 0);
+            else issue_step(tmem, a0 + ks * 256, b0 + ks * 256, 0, 128, 512, c == 0 && ks == 0);
+          }
+          mma_commit(&ss->empty[s]);
+        }
+        if (!ok) break;
+        mma_commit(&ss->acc_full);
+      }
+      // every issued MMA completes before TMEM and shared memory are released
+      mma_commit(&ss->fin);
+      mbar_wait(&ss->fin, 0);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue ----------------
+    const int qd = warp & 3, half = (warp - 2) >> 2;
+    const int row = 32 * qd + lane;
+    const uint32_t addr = tmem + ((uint32_t)(32 * qd) << 16);
+    const int etid = tid - 64;
+    const int vn = min(kSplitN, p.nvecs - p.v0);
+    int nt = 0;
+    for (int t = blockIdx.x; t < L.ntiles; t += gridDim.x, ++nt) {
+      const DevStreamTile T = L.tiles[t];
+      const bool ok = mbar_wait_or_abort(&ss->acc_full, (uint32_t)(nt & 1), abort);
+      if (epi_sync_or(!ok || *abort)) break;
+      fence_after_sync();
+      const int32_t si = L.sidx[(int64_t)t * kSplitM + row];
+      const double rinv = si >= 0 ? L.scales[si].y : 0.0;
+      const double2 *vsc = p.vec_scale + (int64_t)T.vs * kSplitN;
+      for (int v8 = 32 * half; v8 < 32 * half + 32; v8 += 8) {
+        int32_t d[kSplitDiag][8];
+        tmem_ld_diags(addr + v8, d);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) xs[row * kXsStride + v8 + j] = recombine(d, j) * rinv * vsc[v8 + j].y;
+      }
+      // TMEM is free for the next tile once every epilogue warp has read it
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&ss->acc_empty);
+      asm volatile("bar.sync 1, %0;" ::"n"(32 * kStreamEpiWarps));
+      double *dbase = T.buf == 0 ? p.q : T.buf == 1 ? p.xbuf : p.alm_out;
+      for (int r = etid >> 5; r < kSplitM; r += kStreamEpiWarps) {
+        const int32_t dr = L.rows[(int64_t)t * kSplitM + r];
+        const int vv = 2 * lane;
+        if (dr >= 0 && vv < vn)
+          *reinterpret_cast<double2 *>(dbase + (int64_t)dr * p.nvecs + p.v0 + vv) =
+              make_double2(xs[r * kXsStride + vv], xs[r * kXsStride + vv + 1]);
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(32 * kStreamEpiWarps));
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  if (*abort) set_status(p.status, kStatusTimeout);
+  if (warp == 0) tmem_free(tmem);
+}
+
+// ------------------------------------------------------------------------
+// Plan creation: residual P of the split tiles sliced once into A chunks in
+// the layouts the on-the-fly kernels build in shared memory (alm2map
+// K-major, map2alm MN-major), from the same recurrence seeds and scales, so
+// the streamed GEMM sees exactly the slices those kernels would generate.
+// One CTA of 512 threads per tile, all its K chunks.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSplitThr) k_res_slices_a2m(SplitParams p, StreamLaunch L) {
+  const int t = blockIdx.x;
+  const DevSplitTileA T = p.tiles_a[t];
+  const DevStreamTile ST = L.tiles[t];
+  const DevGroup G = p.groups[T.group];
+  const DevSplitGroup S = p.sgroups[T.group];
+  const int tid = threadIdx.x, c = tid & (kSplitM - 1), seg = tid >> 7;
+  const int64_t gc = (int64_t)T.col0 + c;
+  DevGCol C{};
+  double2 csc = make_double2(0.0, 0.0);
+  if (c < T.ncols) {
+    C = p.gcols[G.cols + gc];
+    csc = p.col_scale[G.cols + gc];
+  } else {
+    C.start = G.nrows;
+  }
+  unsigned char *A = reinterpret_cast<unsigned char *>(const_cast<int8_t *>(L.a)) + ST.a * (int64_t)kStageA;
+  for (int kc = T.kc0; kc < S.nrchunks; ++kc) {
+    unsigned char *dst = A + (int64_t)(kc - T.kc0) * kStageA + (c >> 3) * 512 + seg * 128 + (c & 7) * 16;
+    double v[16];
+    if (column_segment(p, G, C, gc, kc * kSplitK + 16 * seg, v)) store_slices(dst, v, &csc.x, 0);
+    else store_zero_slices(dst);
+  }
+}
+
+__global__ void __launch_bounds__(kSplitThr) k_res_slices_m2a(SplitParams p, StreamLaunch L) {
+  __shared__ double2 rsc[kSplitM];
+  const int t = blockIdx.x;
+  const DevSplitTileB T = p.tiles_b[t];
+  const DevStreamTile ST = L.tiles[t];
+  const DevGroup G = p.groups[T.group];
+  const DevSplitGroup S = p.sgroups[T.group];
+  const int tid = threadIdx.x, cl = tid & (kSplitK - 1), seg = tid >> 6;
+  if (tid < kSplitM) rsc[tid] = tid < T.nrows ? p.row_scale[S.rowoff + T.row0 + tid] : make_double2(0.0, 0.0);
+  __syncthreads();
+  const int r0 = T.row0 + 16 * seg;
+  unsigned char *A = reinterpret_cast<unsigned char *>(const_cast<int8_t *>(L.a)) + ST.a * (int64_t)kStageA;
+  for (int kc = 0; kc < S.ncchunks; ++kc) {
+    const int64_t gc = (int64_t)kc * kSplitK + cl;
+    DevGCol C{};
+    if (gc < G.ncols) C = p.gcols[G.cols + gc];
+    else C.start = G.nrows;
+    unsigned char *dst = A + (int64_t)kc * kStageA + seg * 1024 + (cl >> 3) * 128 + (cl & 7) * 16;
+    double v[16];
+    if (column_segment(p, G, C, gc, r0, v)) store_slices(dst, v, &rsc[16 * seg].x, 2);
+    else store_zero_slices(dst);
+  }
+}
+
 }  // namespace
+
+static size_t stream_smem_bytes() {
+  return (size_t)kStreamStages * kStreamStage + 128 + (size_t)kSplitM * kXsStride * 8;
+}
+
+cudaError_t launch_stream(const SplitParams &prm, const StreamLaunch &L, int grid, cudaStream_t st) {
+  if (L.ntiles <= 0) return cudaSuccess;
+  const size_t sm = stream_smem_bytes();
+  cudaError_t e;
+  if (L.a_mn) {
+    e = cudaFuncSetAttribute(k_stream_split<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_stream_split<1><<<grid, kStreamThr, sm, st>>>(prm, L);
+  } else {
+    e = cudaFuncSetAttribute(k_stream_split<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_stream_split<0><<<grid, kStreamThr, sm, st>>>(prm, L);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_slices(const SplitParams &prm, const StreamLaunch &a2m, const StreamLaunch &m2a,
+                                   cudaStream_t st) {
+  if (a2m.ntiles > 0) k_res_slices_a2m<<<a2m.ntiles, kSplitThr, 0, st>>>(prm, a2m);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (m2a.ntiles > 0) k_res_slices_m2a<<<m2a.ntiles, kSplitThr, 0, st>>>(prm, m2a);
+  return cudaGetLastError();
+}
 
 static size_t level_smem_bytes() {
   return (size_t)2 * kLevelStage + 128 + (kSplitN + kSplitM) * 16 + (size_t)kSplitM * kXsStride * 8;

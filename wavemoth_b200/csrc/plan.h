@@ -165,6 +165,21 @@ struct DevSplitLevelTile {  // <= kSplitM rows (z or s) of one root unit
   int32_t unit, row0, nrows, pad;
 };
 
+// One M tile of a streamed split GEMM: every operand chunk is read from
+// global memory (A chunks sliced once per plan, B planes sliced per call),
+// so residual and level products of both directions share one kernel.
+// Output row r of the tile goes to row rows[tile * kSplitM + r] of the
+// destination buffer (-1: none), scaled by 1 / scale of that tile row
+// (entry scale_idx[tile * kSplitM + r] of the launch's scale table).
+struct DevStreamTile {
+  int64_t a;       // first A chunk (kSplitSlices x kSplitM x kSplitK bytes each)
+  int64_t b;       // first B plane (kSplitPlane bytes each)
+  int32_t nk;      // K chunks (> 0)
+  int32_t vs;      // vector-scale row: group, or ngroups + root unit
+  int32_t buf;     // destination: 0 q, 1 X buffer, 2 alm
+  int32_t pad;
+};
+
 // Per ring pair (ring number r from the equator).
 struct DevRing {
   int32_t n;              // pixels in the ring

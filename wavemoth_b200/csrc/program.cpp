@@ -446,6 +446,79 @@ namespace wm {
 // all rows) and depth 1 (every root a (T, B) pair over two leaves, T blocks
 // on rows [0, nk/2), B blocks on [nk/2, nk) -- butterfly.pyx:570-573) are
 // taken; anything else stays with the generic kernels.
+// Streamed split GEMM tables, tile for tile in the order of the split tile
+// lists: residual tiles take consecutive chunks of one A pool (alm2map
+// tiles, then map2alm tiles), level tiles point into the sliced W.  The row
+// maps give each tile row's destination: alm2map residual rows of q (depth
+// 0) or of the X buffer (depth 1), map2alm residual rows of the alm, level
+// rows of q (alm2map) or of the X buffer (map2alm).
+static void build_stream_tables(HostProgram &P) {
+  const int64_t ni = 2 * (int64_t)P.nside;
+  for (int k = 0; k < 4; ++k) {
+    P.stream_tiles[k].clear();
+    P.stream_rows[k].clear();
+    P.stream_sidx[k].clear();
+  }
+  auto add = [&](int k, const DevStreamTile &t, const std::vector<int32_t> &rows, const std::vector<int32_t> &sidx) {
+    P.stream_tiles[k].push_back(t);
+    P.stream_rows[k].insert(P.stream_rows[k].end(), rows.begin(), rows.end());
+    P.stream_sidx[k].insert(P.stream_sidx[k].end(), sidx.begin(), sidx.end());
+  };
+  std::vector<int32_t> rows(kSplitM), sidx(kSplitM);
+  int64_t a = 0;
+  for (const DevSplitTileA &T : P.stiles_a) {
+    const DevGroup &G = P.groups[T.group];
+    const DevSplitGroup &S = P.sgroups[T.group];
+    const DevMatrix &M = P.mats[G.matrix];
+    const int64_t base = G.in_q ? (int64_t)(2 * M.m + M.odd) * ni : (int64_t)M.xrow;
+    for (int r = 0; r < kSplitM; ++r) {
+      const bool act = r < T.ncols;
+      rows[r] = act ? (int32_t)(base + P.gcols[G.cols + T.col0 + r].row) : -1;
+      sidx[r] = act ? (int32_t)(G.cols + T.col0 + r) : -1;
+    }
+    const int32_t nk = S.nrchunks - T.kc0;
+    add(kStreamResA2M, DevStreamTile{a, S.apl + T.kc0, nk, T.group, G.in_q ? 0 : 1, 0}, rows, sidx);
+    a += nk;
+  }
+  for (const DevSplitTileB &T : P.stiles_b) {
+    const DevGroup &G = P.groups[T.group];
+    const DevSplitGroup &S = P.sgroups[T.group];
+    const DevMatrix &M = P.mats[G.matrix];
+    const int64_t arow0 = (int64_t)M.m * (2 * P.lmax - M.m + 3) / 2 + M.odd;
+    for (int r = 0; r < kSplitM; ++r) {
+      const bool act = r < T.nrows;
+      rows[r] = act ? (int32_t)(arow0 + 2 * (int64_t)(G.rs + T.row0 + r)) : -1;
+      sidx[r] = act ? (int32_t)(S.rowoff + T.row0 + r) : -1;
+    }
+    add(kStreamResM2A, DevStreamTile{a, S.xpl, S.ncchunks, T.group, 2, 0}, rows, sidx);
+    a += S.ncchunks;
+  }
+  P.stream_res_achunks = a;
+  const int32_t ng = (int32_t)P.groups.size();
+  for (int dir = 0; dir < 2; ++dir) {
+    const bool a2m = dir == 0;
+    for (const DevSplitLevelTile &T : a2m ? P.stiles_la : P.stiles_lm) {
+      const DevRootUnit &U = P.roots[T.unit];
+      const DevPair &pr = P.pairs[U.pair];
+      const DevMatrix &M = P.mats[U.matrix];
+      const DevSplitRoot &R = P.sroots[T.unit];
+      const int32_t nk = a2m ? R.nsc : R.nzc;
+      for (int r = 0; r < kSplitM; ++r) {
+        const bool act = r < T.nrows;
+        const int32_t rr = T.row0 + r;
+        int64_t dst = -1;
+        if (act && a2m) dst = (int64_t)(2 * M.m + M.odd) * ni + pr.out_left + rr;
+        if (act && !a2m) dst = (int64_t)M.xrow + (rr < pr.kT ? pr.inT + rr : pr.inB + (rr - pr.kT));
+        rows[r] = (int32_t)dst;
+        sidx[r] = act ? (int32_t)((a2m ? R.rs_a2m : R.rs_m2a) + rr) : -1;
+      }
+      const int64_t a0 = (a2m ? R.a_a2m : R.a_m2a) + (int64_t)(T.row0 / kSplitM) * nk;
+      add(a2m ? kStreamLevelA2M : kStreamLevelM2A,
+          DevStreamTile{a0, a2m ? R.b_a2m : R.b_m2a, nk, ng + T.unit, a2m ? 0 : 1, 0}, rows, sidx);
+    }
+  }
+}
+
 // Split-precision residual tables: operand chunk offsets per group and the
 // M tiles of both directions, largest K extent first.
 static void build_split_tables(HostProgram &P) {
@@ -524,6 +597,7 @@ static void build_split_tables(HostProgram &P) {
   P.split_level_achunks = achunks;
   P.split_level_rows = lrows;
   P.split_chunks = std::max(P.split_chunks, std::max(bla, blm));
+  build_stream_tables(P);
 }
 
 bool build_fast_path(HostProgram &P, std::string &err) {

@@ -40,6 +40,11 @@ struct HostProgram {
   std::vector<DevSplitLevelTile> stiles_la, stiles_lm;  // alm2map / map2alm level tiles
   int64_t split_level_achunks = 0;      // A chunks of W, both directions
   int64_t split_level_rows = 0;         // row scales of W, both directions
+  // streamed split GEMM launches (kStream* order): the tiles, and per tile
+  // row its destination row and scale index (-1: padding row)
+  std::vector<DevStreamTile> stream_tiles[4];
+  std::vector<int32_t> stream_rows[4], stream_sidx[4];
+  int64_t stream_res_achunks = 0;       // A chunks of sliced residual P, both directions
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)
@@ -47,6 +52,9 @@ struct HostProgram {
   int64_t rec_columns = 0;       // columns of recurrence strips (x2, P0, P1 each)
   int64_t aux_values = 0;        // recurrence coefficients stored
 };
+
+// Streamed split GEMM launches.
+enum : int { kStreamResA2M = 0, kStreamResM2A = 1, kStreamLevelA2M = 2, kStreamLevelM2A = 3 };
 
 // Builds the tensor-core path tables for matrices of depth 0 and 1.
 bool build_fast_path(HostProgram &P, std::string &err);

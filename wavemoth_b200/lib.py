@@ -17,6 +17,12 @@ WAVEMOTH_MEASURE = 0x1
 WAVEMOTH_NO_RESOURCE_COPY = 0x10
 WAVEMOTH_DEVICE_POINTERS = 0x100
 WAVEMOTH_PRECISION_SPLIT = 0x200
+WAVEMOTH_SPLIT_GENERATE = 0x400
+# precision= of the plans: FP64 tensor cores, or the split int8 path with the
+# residual P sliced once per plan ("split") or generated at every call
+# ("split-generate", less device memory)
+PRECISION_FLAGS = {"double": 0, "split": WAVEMOTH_PRECISION_SPLIT,
+                   "split-generate": WAVEMOTH_PRECISION_SPLIT | WAVEMOTH_SPLIT_GENERATE}
 
 _configured = False
 
@@ -63,7 +69,7 @@ class ShtPlan:
             raise ValueError("Invalid ordering: %s" % ordering)
         if direction not in ("alm2map", "map2alm"):
             raise ValueError("Invalid direction: %s" % direction)
-        if precision not in ("double", "split"):
+        if precision not in PRECISION_FLAGS:
             raise ValueError("Invalid precision: %s" % precision)
         alm, maps = (input, output) if direction == "alm2map" else (output, input)
         if not (isinstance(alm, np.ndarray) and alm.dtype == np.complex128 and alm.ndim == 2
@@ -88,7 +94,7 @@ class ShtPlan:
               else _lib().wavemoth_plan_from_healpix)
         self._plan = fn(Nside, lmax, mmax, self.nmaps, nthreads,
                         input.ctypes.data, output.ctypes.data, WAVEMOTH_MMAJOR,
-                        WAVEMOTH_ESTIMATE | (WAVEMOTH_PRECISION_SPLIT if precision == "split" else 0),
+                        WAVEMOTH_ESTIMATE | PRECISION_FLAGS[precision],
                         None if matrix_data_filename is None else os.fsencode(matrix_data_filename))
         if not self._plan:
             raise WavemothError("Plan creation failed: " + last_error())

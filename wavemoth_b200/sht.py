@@ -10,14 +10,15 @@ import os
 import torch
 
 from . import _native
-from .lib import (WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WAVEMOTH_PRECISION_SPLIT, WavemothError,
-                  last_error)
+from .lib import PRECISION_FLAGS, WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WavemothError, last_error
 
 
 class Transform:
     """Both directions share one device plan (the compiled butterfly program
     serves A^T for alm2map and A for map2alm).  precision='split' runs the
-    residual products as sliced int8 tensor-core GEMMs re-summed in FP64."""
+    residual and level products as sliced int8 tensor-core GEMMs re-summed in
+    FP64 ('split-generate': the residual P regenerated at every call instead
+    of held sliced in device memory)."""
 
     def __init__(self, resource_file, nside, lmax, nmaps=1, precision="double"):
         if not torch.cuda.is_available():
@@ -26,10 +27,10 @@ class Transform:
         self.npix = 12 * nside * nside
         self.nalm = (lmax + 1) * (lmax + 2) // 2
         self.resource_file = resource_file
-        if precision not in ("double", "split"):
-            raise ValueError("precision must be 'double' or 'split'")
+        if precision not in PRECISION_FLAGS:
+            raise ValueError("precision must be one of %s" % ", ".join(PRECISION_FLAGS))
         self.precision = precision
-        flags = WAVEMOTH_DEVICE_POINTERS | (WAVEMOTH_PRECISION_SPLIT if precision == "split" else 0)
+        flags = WAVEMOTH_DEVICE_POINTERS | PRECISION_FLAGS[precision]
         lib = _native.lib()
         p = lib.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR,
                                          flags, os.fsencode(resource_file))
