@@ -116,9 +116,10 @@ cudaError_t launch_stream(const SplitParams &prm, const StreamLaunch &L, int gri
 cudaError_t launch_residual_slices(const SplitParams &prm, const StreamLaunch &a2m, const StreamLaunch &m2a,
                                    cudaStream_t st);
 
-// which: 0 alm operand slices, 1 alm2map residual, 2 X operand slices, 3 map2alm residual,
-//        4 alm2map level operand (X) slices, 5 alm2map level GEMM,
-//        6 map2alm level operand (q~) slices, 7 map2alm level GEMM
+// which: 0 alm operand slices, 1 alm2map residual (P generated in the kernel),
+//        2 X operand slices, 3 map2alm residual (P generated in the kernel),
+//        4 alm2map level operand (X) slices, 6 map2alm level operand (q~) slices;
+// the level GEMMs and the residual GEMMs on sliced P run as launch_stream.
 cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream_t st);
 // Plan creation: P scales of both directions, and the sliced W of the levels.
 cudaError_t launch_split_scales(const SplitParams &prm, cudaStream_t st);

@@ -36,12 +36,20 @@
 // the recurrence seeds stored every kSeedRows rows, and writes each slice of
 // it as one 16-byte store in both layouts.  512 producer threads per CTA.
 //
-// Pipeline: two stages.  All threads produce chunk t into stage t % 2 while
-// the tensor core still works on chunk t - 1; one thread issues the MMAs of
-// a stage and commits them to that stage's mbarrier, which the producers
-// wait on before refilling the stage.  Every wait is bounded: on expiry the
-// kernel records kStatusTimeout, stops issuing work, waits (bounded) for
-// its MMAs, frees its TMEM and returns.
+// Two ways to feed A:
+//   * stored (default): the residual P of every tile is sliced once per plan
+//     (k_res_slices_*) into device memory, and k_stream_split streams A and
+//     B chunks with bulk copies; the level products (W sliced once per plan
+//     by k_level_slices) always run this way;
+//   * generated (WAVEMOTH_SPLIT_GENERATE, or too little device memory):
+//     k_a2m_split / k_m2a_split produce P in the CTA.  Two stages: all
+//     threads produce chunk t into stage t % 2 while the tensor core still
+//     works on chunk t - 1; one thread issues the MMAs of a stage and commits
+//     them to that stage's mbarrier, which the producers wait on before
+//     refilling the stage.
+// Both give the same slices and the same int32 accumulators.  Every wait is
+// bounded: on expiry the kernel records kStatusTimeout, stops issuing work,
+// waits (bounded) for its MMAs and copies, frees its TMEM and returns.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -788,22 +796,8 @@ __global__ void __launch_bounds__(kSplitM) k_level_slices(SplitParams p) {
   }
 }
 
-// ------------------------------------------------------------------------
-// Level GEMM, split precision.  Unit = one level tile (<= 128 rows of one
-// root's W), K chunks of 64.  Both operands arrive pre-sliced: thread 0
-// copies each chunk with 1D bulk (TMA) copies completing on the stage's
-// mbarrier, two stages, and issues the MMAs; the next tile's first chunk is
-// fetched while the CTA drains the accumulators.
-// ------------------------------------------------------------------------
-constexpr int kLevelThr = 256;
-constexpr int kLevelStage = kStageA + kStageB;  // 73728 bytes
-
-struct LevelSmem {
-  uint64_t full[2], empty[2], acc;
-  uint32_t tmem;
-  int32_t abort;
-};
-
+// One-dimensional bulk copy (TMA, no multicast) completing on `bar`, and the
+// arrival that announces its bytes.
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -815,170 +809,6 @@ __device__ __forceinline__ void expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
-
-template <bool kA2M>
-struct LevelTile {
-  DevSplitLevelTile T;
-  DevSplitRoot R;
-  int nk;
-  int64_t abase, bbase;
-};
-
-template <bool kA2M>
-__device__ __forceinline__ LevelTile<kA2M> level_tile(const SplitParams &p, int unit) {
-  LevelTile<kA2M> L;
-  L.T = kA2M ? p.tiles_la[unit] : p.tiles_lm[unit];
-  L.R = p.sroots[L.T.unit];
-  L.nk = kA2M ? L.R.nsc : L.R.nzc;
-  L.abase = (kA2M ? L.R.a_a2m : L.R.a_m2a) + (int64_t)(L.T.row0 / kSplitM) * L.nk;
-  L.bbase = kA2M ? L.R.b_a2m : L.R.b_m2a;
-  return L;
-}
-
-// Chunk c of tile L into stage (g & 1) (thread 0): waits for the MMAs that
-// last read the stage (its use g >> 1 - 1), then two bulk copies.
-template <bool kA2M>
-__device__ __forceinline__ bool level_load(const SplitParams &p, unsigned char *smem, LevelSmem *ls,
-                                           const LevelTile<kA2M> &L, int c, long long g) {
-  const int s = (int)(g & 1);
-  const long long use = g >> 1;
-  if (use > 0 && !mbar_wait(&ls->empty[s], (uint32_t)((use - 1) & 1))) return false;
-  const uint32_t dst = smem_u32(smem + s * kLevelStage);
-  expect_tx(&ls->full[s], kLevelStage);
-  bulk_load(dst, p.level_a + (L.abase + c) * (int64_t)kStageA, kStageA, &ls->full[s]);
-  bulk_load(dst + kStageA, p.planes + (L.bbase + c) * (int64_t)kSplitPlane, kStageB, &ls->full[s]);
-  return true;
-}
-
-template <bool kA2M>
-__global__ void __launch_bounds__(kLevelThr, 1) k_level_split(SplitParams p) {
-  extern __shared__ __align__(1024) unsigned char smem[];
-  LevelSmem *ls = reinterpret_cast<LevelSmem *>(smem + 2 * kLevelStage);
-  double2 *vsc = reinterpret_cast<double2 *>(smem + 2 * kLevelStage + 128);
-  double2 *rsc = vsc + kSplitN;
-  double *xs = reinterpret_cast<double *>(smem + 2 * kLevelStage + 128 + (kSplitN + kSplitM) * 16);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ntiles = kA2M ? p.ntiles_la : p.ntiles_lm;
-  if (warp == 0) tmem_alloc(&ls->tmem);
-  if (tid == 0) {
-    for (int s = 0; s < 2; ++s) {
-      mbar_init(&ls->full[s], 1);
-      mbar_init(&ls->empty[s], 1);
-    }
-    mbar_init(&ls->acc, 1);
-    ls->abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = ls->tmem;
-  long long g = 0;        // chunks loaded so far (thread 0)
-  uint32_t acc_phase = 0;
-  bool prefetched = false;
-  for (int unit = blockIdx.x; unit < ntiles; unit += gridDim.x) {
-    const LevelTile<kA2M> L = level_tile<kA2M>(p, unit);
-    const DevRootUnit U = p.roots[L.T.unit];
-    const DevPair P = p.pairs[U.pair];
-    const DevMatrix M = p.mats[U.matrix];
-    if (tid < kSplitN) vsc[tid] = p.vec_scale[((int64_t)p.ngroups + L.T.unit) * kSplitN + tid];
-    if (tid < kSplitM)
-      rsc[tid] = tid < L.T.nrows ? p.level_rs[(kA2M ? L.R.rs_a2m : L.R.rs_m2a) + L.T.row0 + tid]
-                                 : make_double2(0.0, 0.0);
-    if (tid == 0) {
-      bool ok = true;
-      long long g0 = g;
-      if (!prefetched) {
-        ok = level_load<kA2M>(p, smem, ls, L, 0, g++);
-      } else {
-        g0 = g - 1;
-      }
-      prefetched = false;
-      for (int c = 0; c < L.nk && ok; ++c) {
-        const long long gc = g0 + c;
-        if (c + 1 < L.nk) ok = level_load<kA2M>(p, smem, ls, L, c + 1, g++);
-        const int s = (int)(gc & 1);
-        if (ok) ok = mbar_wait(&ls->full[s], (uint32_t)((gc >> 1) & 1));
-        if (!ok) break;
-        fence_after_sync();
-        const uint32_t a0 = smem_u32(smem + s * kLevelStage), b0 = a0 + kStageA;
-        for (int ks = 0; ks < kSplitK / 32; ++ks)
-          issue_step(tmem, a0 + ks * 256, b0 + ks * 256, 0, 128, 512, c == 0 && ks == 0);
-        mma_commit(&ls->empty[s]);
-      }
-      if (ok) mma_commit(&ls->acc);
-      else ls->abort = 1;
-    }
-    __syncthreads();
-    if (ls->abort) break;
-    const bool ok = mbar_wait(&ls->acc, acc_phase);
-    acc_phase ^= 1u;
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) ls->abort = 1;
-      break;
-    }
-    fence_after_sync();
-    // prefetch the next tile's first chunk while the accumulators drain
-    if (tid == 0 && unit + (int)gridDim.x < ntiles) {
-      const LevelTile<kA2M> Ln = level_tile<kA2M>(p, unit + gridDim.x);
-      if (Ln.nk > 0) {
-        prefetched = level_load<kA2M>(p, smem, ls, Ln, 0, g++);
-        if (!prefetched) ls->abort = 1;
-      }
-    }
-    // epilogue: TMEM lane = tile row; warps w and w + 4 share a lane quarter
-    {
-      const int row = 32 * (warp & 3) + lane;
-      const double rinv = rsc[row].y;
-      const uint32_t addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-      for (int v8 = (warp >> 2) * 32; v8 < (warp >> 2) * 32 + 32; v8 += 8) {
-        int32_t d[kSplitDiag][8];
-#pragma unroll
-        for (int k = 0; k < kSplitDiag; ++k) tmem_ld8(addr + 64 * k + v8, d[k]);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) xs[row * kXsStride + v8 + j] = recombine(d, j) * rinv * vsc[v8 + j].y;
-      }
-    }
-    fence_before_sync();
-    __syncthreads();
-    {
-      const int vn = min(kSplitN, p.nvecs - p.v0);
-      const int vv = 2 * lane;
-      for (int r = warp; r < L.T.nrows; r += kLevelThr / 32) {
-        const int rr = L.T.row0 + r;
-        double *dst;
-        if (kA2M) {
-          dst = p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs + (int64_t)(P.out_left + rr) * p.nvecs;
-        } else {
-          const int xr = rr < P.kT ? P.inT + rr : P.inB + (rr - P.kT);
-          dst = p.xbuf + (M.xrow + xr) * p.nvecs;
-        }
-        if (vv < vn)
-          *reinterpret_cast<double2 *>(dst + p.v0 + vv) =
-              make_double2(xs[r * kXsStride + vv], xs[r * kXsStride + vv + 1]);
-      }
-    }
-    __syncthreads();
-    if (ls->abort) break;
-  }
-  if (ls->abort) {
-    set_status(p.status, kStatusTimeout);
-    if (tid == 0) {
-      // bounded waits for this CTA's copies and MMAs still in flight
-      for (int s = 0; s < 2; ++s) {
-        const long long gl = (g - 1) - (((g - 1) - s) & 1);  // last chunk loaded into stage s
-        if (gl >= 0) mbar_wait(&ls->full[s], (uint32_t)((gl >> 1) & 1));
-      }
-      mma_commit(&ls->acc);
-      mbar_wait(&ls->acc, acc_phase);
-    }
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  if (warp == 0) tmem_free(tmem);
-}
-
 
 // ------------------------------------------------------------------------
 // Streamed split GEMM.  Both operands arrive pre-sliced from global memory
@@ -1065,6 +895,9 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
   extern __shared__ __align__(1024) unsigned char smem[];
   StreamSmem *ss = reinterpret_cast<StreamSmem *>(smem + kStreamStages * kStreamStage);
   double *xs = reinterpret_cast<double *>(smem + kStreamStages * kStreamStage + 128);
+  double *erinv = xs + kSplitM * kXsStride;  // epilogue: 1 / scale of each tile row,
+  double *evs = erinv + kSplitM;             // 1 / scale of each vector,
+  int32_t *erow = reinterpret_cast<int32_t *>(evs + kSplitN);  // destination row of each tile row
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int32_t *abort = &ss->abort;
   if (warp == 0) tmem_alloc(&ss->tmem);
@@ -1087,8 +920,11 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
     // ---------------- loader ----------------
     if (lane == 0) {
       long long g = 0;  // chunks issued
+      DevStreamTile Tn{};
+      if (blockIdx.x < L.ntiles) Tn = L.tiles[blockIdx.x];
       for (int t = blockIdx.x; t < L.ntiles && !*abort; t += gridDim.x) {
-        const DevStreamTile T = L.tiles[t];
+        const DevStreamTile T = Tn;
+        if (t + (int)gridDim.x < L.ntiles) Tn = L.tiles[t + gridDim.x];  // next descriptor in flight
         for (int c = 0; c < T.nk; ++c, ++g) {
           const int s = (int)(g % kStreamStages);
           const long long use = g / kStreamStages;
@@ -1148,17 +984,25 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
     int nt = 0;
     for (int t = blockIdx.x; t < L.ntiles; t += gridDim.x, ++nt) {
       const DevStreamTile T = L.tiles[t];
+      // the tile's row map and scales, fetched while its MMAs still run (the
+      // previous tile's rows were all written before the last barrier)
+      if (etid < kSplitM) {
+        const int64_t e = (int64_t)t * kSplitM + etid;
+        erow[etid] = L.rows[e];
+        const int32_t si = L.sidx[e];
+        erinv[etid] = si >= 0 ? L.scales[si].y : 0.0;
+      } else if (etid < kSplitM + kSplitN) {
+        evs[etid - kSplitM] = p.vec_scale[(int64_t)T.vs * kSplitN + etid - kSplitM].y;
+      }
       const bool ok = mbar_wait_or_abort(&ss->acc_full, (uint32_t)(nt & 1), abort);
       if (epi_sync_or(!ok || *abort)) break;
       fence_after_sync();
-      const int32_t si = L.sidx[(int64_t)t * kSplitM + row];
-      const double rinv = si >= 0 ? L.scales[si].y : 0.0;
-      const double2 *vsc = p.vec_scale + (int64_t)T.vs * kSplitN;
+      const double rinv = erinv[row];
       for (int v8 = 32 * half; v8 < 32 * half + 32; v8 += 8) {
         int32_t d[kSplitDiag][8];
         tmem_ld_diags(addr + v8, d);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) xs[row * kXsStride + v8 + j] = recombine(d, j) * rinv * vsc[v8 + j].y;
+        for (int j = 0; j < 8; ++j) xs[row * kXsStride + v8 + j] = recombine(d, j) * rinv * evs[v8 + j];
       }
       // TMEM is free for the next tile once every epilogue warp has read it
       fence_before_sync();
@@ -1167,7 +1011,7 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
       asm volatile("bar.sync 1, %0;" ::"n"(32 * kStreamEpiWarps));
       double *dbase = T.buf == 0 ? p.q : T.buf == 1 ? p.xbuf : p.alm_out;
       for (int r = etid >> 5; r < kSplitM; r += kStreamEpiWarps) {
-        const int32_t dr = L.rows[(int64_t)t * kSplitM + r];
+        const int32_t dr = erow[r];
         const int vv = 2 * lane;
         if (dr >= 0 && vv < vn)
           *reinterpret_cast<double2 *>(dbase + (int64_t)dr * p.nvecs + p.v0 + vv) =
@@ -1242,7 +1086,8 @@ __global__ void __launch_bounds__(kSplitThr) k_res_slices_m2a(SplitParams p, Str
 }  // namespace
 
 static size_t stream_smem_bytes() {
-  return (size_t)kStreamStages * kStreamStage + 128 + (size_t)kSplitM * kXsStride * 8;
+  return (size_t)kStreamStages * kStreamStage + 128 + (size_t)kSplitM * kXsStride * 8 +
+         (kSplitM + kSplitN) * sizeof(double) + kSplitM * sizeof(int32_t);
 }
 
 cudaError_t launch_stream(const SplitParams &prm, const StreamLaunch &L, int grid, cudaStream_t st) {
@@ -1268,10 +1113,6 @@ cudaError_t launch_residual_slices(const SplitParams &prm, const StreamLaunch &a
   if (e != cudaSuccess) return e;
   if (m2a.ntiles > 0) k_res_slices_m2a<<<m2a.ntiles, kSplitThr, 0, st>>>(prm, m2a);
   return cudaGetLastError();
-}
-
-static size_t level_smem_bytes() {
-  return (size_t)2 * kLevelStage + 128 + (kSplitN + kSplitM) * 16 + (size_t)kSplitM * kXsStride * 8;
 }
 
 cudaError_t launch_level_slices(const SplitParams &prm, cudaStream_t st) {
@@ -1315,20 +1156,6 @@ cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream
     case 6:
       k_split_operand_level<3><<<grid, 256, 0, st>>>(prm);
       break;
-    case 5:
-    case 7: {
-      const size_t sm = level_smem_bytes();
-      if (which == 5) {
-        e = cudaFuncSetAttribute(k_level_split<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        k_level_split<true><<<grid, kLevelThr, sm, st>>>(prm);
-      } else {
-        e = cudaFuncSetAttribute(k_level_split<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        k_level_split<false><<<grid, kLevelThr, sm, st>>>(prm);
-      }
-      break;
-    }
     default:
       return cudaErrorInvalidValue;
   }
