@@ -154,14 +154,20 @@ struct RingParams {
   int32_t ntasks;
   int32_t smem;           // bytes
   int32_t nphase_hi;      // entries of the coarse phase table (mmax / 64 + 1)
+  // per ring pair, kPhaseLo + nphase_hi phase factors (fine then coarse
+  // table), computed at plan creation
+  const double2 *phases;
+  double2 *phases_out;
 };
 
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
-                              double *aux, cudaStream_t st);
-// Shared-memory bytes of a ring CTA whose transform buffer holds `cplx`
-// complex values per map lane times the lanes.
+                              double *aux, double2 *phases, cudaStream_t st);
+constexpr int32_t kRingPhaseLo = 64;  // fine phase table entries per ring
+// Shared-memory bytes of a ring CTA whose transform buffer holds
+// `buffer_cplx` complex values (transform length times lanes), with its
+// phase tables.
 int32_t ring_cta_smem(int64_t buffer_cplx, int32_t nphase_hi);
 constexpr int32_t kRingBufferCplx = 8192;  // transform buffer of one CTA: 128 KB
 

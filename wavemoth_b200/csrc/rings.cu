@@ -63,7 +63,7 @@ namespace {
 
 constexpr int kRadixLog = 4;           // largest pass radix 2^kRadixLog
 constexpr int kRingThreads = 512;      // 16 points per thread of a kRingBufferCplx buffer
-constexpr int kPhaseLo = 64;           // e^{i m phi0} = hi[m / 64] * lo[m % 64]
+constexpr int kPhaseLo = kRingPhaseLo;  // e^{i m phi0} = hi[m / 64] * lo[m % 64]
 
 struct cplx {
   double x, y;
@@ -80,6 +80,9 @@ __device__ __forceinline__ cplx mul_i(cplx a) { return {-a.y, a.x}; }
 __device__ __forceinline__ cplx ld2(const double *p) {
   const double2 v = *reinterpret_cast<const double2 *>(p);
   return {v.x, v.y};
+}
+__device__ __forceinline__ void st2(double *p, double x, double y) {
+  *reinterpret_cast<double2 *>(p) = make_double2(x, y);
 }
 
 __device__ __forceinline__ unsigned bitrev(unsigned k, int bits) {
@@ -342,14 +345,15 @@ __device__ __forceinline__ cplx ring_chirp(const RingParams &p, const DevRing &R
 }
 
 // Phase factor tables of one ring: lo[b] = e^{i b phi0}, hi[a] = e^{i 64 a phi0}
-// (all ones when phase shifting is off or phi0 = 0).
-__device__ void phase_tables(cplx *lo, cplx *hi, const RingParams &p, const DevRing &R) {
-  const bool on = p.phase_shifts && R.phi_num != 0;
+// (all ones when phase shifting is off or phi0 = 0), copied into shared
+// memory from the per-ring table made at plan creation (k_ring_phases).
+__device__ void phase_tables(cplx *lo, cplx *hi, const RingParams &p, int ring) {
+  const bool on = p.phase_shifts != 0;
+  const double2 *src = p.phases + (int64_t)ring * (kPhaseLo + p.nphase_hi);
   for (int k = threadIdx.x; k < kPhaseLo + p.nphase_hi; k += blockDim.x) {
-    const long long m = k < kPhaseLo ? k : (long long)(k - kPhaseLo) * kPhaseLo;
-    const cplx v = on ? expi_pi(m * R.phi_num, R.phi_den) : cplx{1.0, 0.0};
-    if (k < kPhaseLo) lo[k] = v;
-    else hi[k - kPhaseLo] = v;
+    const double2 t = on ? src[k] : make_double2(1.0, 0.0);
+    if (k < kPhaseLo) lo[k] = {t.x, t.y};
+    else hi[k - kPhaseLo] = {t.x, t.y};
   }
 }
 
@@ -425,7 +429,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
-  phase_tables(plo, phi, p, c.R);
+  phase_tables(plo, phi, p, c.ring);
   __syncthreads();
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   const double *qbase = p.q + (int64_t)c.ring * p.nvecs + 2 * c.map0;
@@ -522,7 +526,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   cplx *buf = reinterpret_cast<cplx *>(smem_d);
   cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
-  phase_tables(plo, phi, p, c.R);
+  phase_tables(plo, phi, p, c.ring);
   const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
   double *qbase = p.q_out + (int64_t)c.ring * p.nvecs + 2 * c.map0;
   const Radices rs = radices(M);
@@ -598,21 +602,33 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
       if (c.two) {
         // both hemispheres: q~_even = g_N + g_S, q~_odd = g_N - g_S (g_S = 0 at the equator)
         const cplx gN = fold(m, mi), gS = fold(m, (1 << c.lgm) | mi);
-        *reinterpret_cast<double2 *>(qe) = make_double2(gN.x + gS.x, gN.y + gS.y);
-        *reinterpret_cast<double2 *>(qo) = make_double2(gN.x - gS.x, gN.y - gS.y);
+        st2(qe, gN.x + gS.x, gN.y + gS.y);
+        st2(qo, gN.x - gS.x, gN.y - gS.y);
       } else {
         const cplx gv = fold(m, mi);
         if (side == 0) {
-          *reinterpret_cast<double2 *>(qe) = make_double2(gv.x, gv.y);
-          *reinterpret_cast<double2 *>(qo) = make_double2(gv.x, gv.y);
+          st2(qe, gv.x, gv.y);
+          st2(qo, gv.x, gv.y);
         } else {
           const cplx e = ld2(qe), o = ld2(qo);
-          *reinterpret_cast<double2 *>(qe) = make_double2(e.x + gv.x, e.y + gv.y);
-          *reinterpret_cast<double2 *>(qo) = make_double2(o.x - gv.x, o.y - gv.y);
+          st2(qe, e.x + gv.x, e.y + gv.y);
+          st2(qo, o.x - gv.x, o.y - gv.y);
         }
       }
     }
     __syncthreads();
+  }
+}
+
+// Plan creation: per ring pair the phase factors e^{i m phi0} for m < 64 and
+// m = 64 a, a < nphase_hi (ones when phi0 = 0).
+__global__ void k_ring_phases(RingParams p) {
+  const DevRing R = p.rings[blockIdx.x];
+  double2 *dst = p.phases_out + (int64_t)blockIdx.x * (kPhaseLo + p.nphase_hi);
+  for (int k = threadIdx.x; k < kPhaseLo + p.nphase_hi; k += blockDim.x) {
+    const long long m = k < kPhaseLo ? k : (long long)(k - kPhaseLo) * kPhaseLo;
+    const cplx v = R.phi_num != 0 ? expi_pi(m * R.phi_num, R.phi_den) : cplx{1.0, 0.0};
+    dst[k] = make_double2(v.x, v.y);
   }
 }
 
@@ -687,11 +703,14 @@ cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
 }
 
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters, double *aux,
-                              cudaStream_t st) {
+                              double2 *phases, cudaStream_t st) {
   k_twiddles<<<64, 256, 0, st>>>(reinterpret_cast<double2 *>(twiddles), prm.twlen);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || !filters) return e;
+  if (e != cudaSuccess) return e;
   RingParams q = prm;
+  q.phases_out = phases;
+  k_ring_phases<<<prm.ni, 128, 0, st>>>(q);
+  if ((e = cudaGetLastError()) != cudaSuccess || !filters) return e;
   q.twiddles = reinterpret_cast<const double2 *>(twiddles);
   q.filters_out = filters;
   q.aux_out = aux;
