@@ -398,11 +398,26 @@ __device__ __forceinline__ bool lane_live(const RingCta &c, int g, int side) {
   return lane_map(c, g) < c.nm && !(lane_side(c, g, side) == 1 && c.ring == 0);
 }
 
+// q values (even part a, odd part b) of the first term of the aliasing sums
+// of bin j, m = j (zero when j > mmax).  Loaded for a batch of bins before
+// any is summed, so that a thread has its q loads in flight together.
+__device__ __forceinline__ void first_term(const double *qg, int j, int mmax, int64_t qstride, int64_t half,
+                                           bool live, cplx &a, cplx &b) {
+  if (live && j <= mmax) {
+    a = ld2(qg + j * qstride);
+    b = ld2(qg + j * qstride + half);
+  } else {
+    a = {0.0, 0.0};
+    b = {0.0, 0.0};
+  }
+}
+
 // Even and odd partial sums of W[j] of one map (q row pointer `qg` at ring r,
-// map g): W = A + B on the northern ring, A - B on the southern one; the
-// aliasing sum runs in increasing m.
+// map g; a0, b0 the q values at m = j): W = A + B on the northern ring,
+// A - B on the southern one; the aliasing sum runs in increasing m.
 __device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int mmax, int64_t qstride,
-                                           int64_t half, const cplx *plo, const cplx *phi, cplx &A, cplx &B) {
+                                           int64_t half, const cplx *plo, const cplx *phi, cplx a0, cplx b0,
+                                           cplx &A, cplx &B) {
   A = {0.0, 0.0};
   B = {0.0, 0.0};
   for (int base = 0;; base += n) {
@@ -410,8 +425,9 @@ __device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int m
     if (m1 > mmax) break;
     {
       const cplx ph = phase_at(plo, phi, m1);
-      A = cadd(A, cmul(ld2(qg + m1 * qstride), ph));
-      B = cadd(B, cmul(ld2(qg + m1 * qstride + half), ph));
+      const cplx a = base ? ld2(qg + m1 * qstride) : a0, b = base ? ld2(qg + m1 * qstride + half) : b0;
+      A = cadd(A, cmul(a, ph));
+      B = cadd(B, cmul(b, ph));
     }
     const int m2 = base + n - j;
     if (m2 <= mmax) {
@@ -421,6 +437,8 @@ __device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int m
     }
   }
 }
+
+constexpr int kGatherBatch = 2;  // bins per thread whose first q loads are issued together (2 measured best)
 
 __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p) {
   extern __shared__ double smem_d[];
@@ -442,35 +460,50 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
     if (side == 1 && c.ring == 0) break;  // the equator is written once
     // Z[k] and Z[N - k] (natural order, chirped for Bluestein rings) of the
     // CTA's hemispheres, from W[k] and W[N - k]
-    const int npairs = (N >> 1) + 1;
-    for (int t = threadIdx.x; t < (npairs << c.lgm); t += blockDim.x) {
-      const int mi = t & gmm, kk = t >> c.lgm, kr = N - kk;
-      cplx Aa = {0.0, 0.0}, Ba = {0.0, 0.0}, Ab = {0.0, 0.0}, Bb = {0.0, 0.0};  // at kk and N - kk
-      if (mi < c.nm) {
+    const int npairs = (N >> 1) + 1, nitems = npairs << c.lgm;
+    for (int t0 = threadIdx.x; t0 < nitems; t0 += kGatherBatch * blockDim.x) {
+      cplx qa[kGatherBatch][2], qb[kGatherBatch][2];  // first-term q at kk and N - kk
+#pragma unroll
+      for (int u = 0; u < kGatherBatch; ++u) {
+        const int t = t0 + u * blockDim.x;
+        const int mi = t & gmm, kk = t >> c.lgm;
+        const bool live = t < nitems && mi < c.nm;
         const double *qg = qbase + 2 * mi;
-        alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, Aa, Ba);
-        if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, Ab, Bb);
-        else { Ab = Aa; Bb = Ba; }
+        first_term(qg, kk, p.mmax, qstride, half, live, qa[u][0], qb[u][0]);
+        first_term(qg, N - kk, p.mmax, qstride, half, live && N - kk != kk, qa[u][1], qb[u][1]);
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (h == 1 && !c.two) break;
-        const int sd = c.two ? h : side;
-        const double sgn = sd ? -1.0 : 1.0;
-        const int g = (h << c.lgm) | mi;
-        const cplx Wa = {Aa.x + sgn * Ba.x, Aa.y + sgn * Ba.y}, Wb = {Ab.x + sgn * Bb.x, Ab.y + sgn * Bb.y};
+      for (int u = 0; u < kGatherBatch; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t >= nitems) break;
+        const int mi = t & gmm, kk = t >> c.lgm, kr = N - kk;
+        cplx Aa = {0.0, 0.0}, Ba = {0.0, 0.0}, Ab = {0.0, 0.0}, Bb = {0.0, 0.0};  // at kk and N - kk
+        if (mi < c.nm) {
+          const double *qg = qbase + 2 * mi;
+          alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, qa[u][0], qb[u][0], Aa, Ba);
+          if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, qa[u][1], qb[u][1], Ab, Bb);
+          else { Ab = Aa; Bb = Ba; }
+        }
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int k = e ? kr : kk;
-          if (e && (kr == kk || kr == N)) break;
-          cplx Wk = e ? Wb : Wa, Wc = cconj(e ? Wa : Wb);
-          if (k == 0) {
-            Wk.y = 0.0;
-            Wc.y = 0.0;
+        for (int h = 0; h < 2; ++h) {
+          if (h == 1 && !c.two) break;
+          const int sd = c.two ? h : side;
+          const double sgn = sd ? -1.0 : 1.0;
+          const int g = (h << c.lgm) | mi;
+          const cplx Wa = {Aa.x + sgn * Ba.x, Aa.y + sgn * Ba.y}, Wb = {Ab.x + sgn * Bb.x, Ab.y + sgn * Bb.y};
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int k = e ? kr : kk;
+            if (e && (kr == kk || kr == N)) break;
+            cplx Wk = e ? Wb : Wa, Wc = cconj(e ? Wa : Wb);
+            if (k == 0) {
+              Wk.y = 0.0;
+              Wc.y = 0.0;
+            }
+            const cplx sm = cadd(Wk, Wc), d = csub(Wk, Wc);
+            const cplx Z = cadd(sm, mul_i(cmul(ring_root(p, c.R, k), d)));
+            buf[at(k, g, lg)] = c.pow2 ? Z : cmul(Z, ring_chirp(p, c.R, k));
           }
-          const cplx sm = cadd(Wk, Wc), d = csub(Wk, Wc);
-          const cplx Z = cadd(sm, mul_i(cmul(ring_root(p, c.R, k), d)));
-          buf[at(k, g, lg)] = c.pow2 ? Z : cmul(Z, ring_chirp(p, c.R, k));
         }
       }
     }
