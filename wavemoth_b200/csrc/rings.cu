@@ -567,6 +567,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   const int gmm = (1 << c.lgm) - 1;
+  const bool npow2 = (n & (n - 1)) == 0;  // every belt ring when nside is a power of two
   for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;
     auto in_row = [&](int g, int64_t pix) -> const double * {
@@ -614,7 +615,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
     // fold the spectrum F[k] (k <= N, from Z in natural order) of a lane into
     // g_m = F[m mod n] or its mirror, times e^{-i m phi0} and the scale
     auto fold = [&](int m, int g) -> cplx {
-      const int jm = m % n;
+      const int jm = npow2 ? (m & (n - 1)) : m % n;
       const bool mirror = jm > N;
       const int k = mirror ? n - jm : jm;
       const int k1 = k == N ? 0 : k, k2 = k == 0 ? 0 : N - k;
