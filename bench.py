@@ -51,6 +51,12 @@ def parse():
     ap.add_argument("--precision", default="split", choices=["split", "double"],
                     help="split: sliced int8 tensor-core residual products (the plain FP64 path "
                          "is timed beside it and is the error reference); double: plain FP64 only")
+    ap.add_argument("--uneven", action="store_true",
+                    help="uneven batch instead of the headline workload: --requests seeded requests "
+                         "(nside from --uneven-nsides, lmax = 2 nside, 1-8 maps, split alm2map) as one "
+                         "graph launch, against the same requests called one after another")
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--uneven-nsides", default="64,128,256,512")
     ap.add_argument("--check", action="store_true",
                     help="also report the round-trip relative error of map 0 vs the FP64 oracle "
                          "at a reduced size (slow on CPU)")
@@ -532,10 +538,79 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+def run_uneven(a):
+    """Uneven batch: every request its own plan (nside, 1-8 maps), all
+    alm2map in split precision, captured into one graph by
+    wavemoth_b200.batch.Batch; timed against calling the same requests one
+    after another on one stream.  Device-resident inputs; L2 is flushed
+    between timed launches."""
+    import types
+
+    import torch
+    from wavemoth_b200.batch import Batch
+    from wavemoth_b200.sht import Transform
+
+    rng = np.random.default_rng(2024)
+    nsides = [int(x) for x in a.uneven_nsides.split(",")]
+    reqs, transforms = [], []
+    total_maps = 0
+    for i in range(a.requests):
+        nside = int(rng.choice(nsides))
+        nmaps = int(rng.integers(1, 9))
+        pa = types.SimpleNamespace(nside=nside, lmax=2 * nside, eps=a.eps, chunk=a.chunk, memop=a.memop,
+                                   plan_dir=a.plan_dir)
+        T = Transform(ensure_plan(pa, 0), nside, 2 * nside, nmaps, precision="split")
+        alm = torch.from_numpy(synthetic_alm(2 * nside, nmaps, 1000 * i)).cuda()
+        out = torch.empty((T.npix, nmaps), dtype=torch.float64, device="cuda")
+        reqs.append((T, "alm2map", alm, out))
+        transforms.append(T)
+        total_maps += nmaps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # larger than L2
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(a.steps):
+            flush.add_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / a.steps
+
+    def sequential():
+        for T, _, alm, out in reqs:
+            T.alm2map(alm, out=out)
+
+    seq_ms = timed(sequential)
+    B = Batch(reqs)
+    width, _ = B.info()
+    batch_ms = timed(B.execute)
+    for T in transforms:
+        T.device_status()
+    line = {"metric": "uneven batch alm2map maps/sec (split precision, one graph launch)",
+            "value": total_maps / (batch_ms / 1e3), "unit": "maps/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": batch_ms, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "uneven batch", "requests": a.requests, "nsides": nsides,
+                       "lmax": "2 nside", "maps_per_request": "1-8 (seeded)", "total_maps": total_maps,
+                       "graph_branches": width, "l2": "flushed between timed launches"},
+            "sequential": {"value": total_maps / (seq_ms / 1e3), "unit": "maps/s", "ms_per_step": seq_ms}}
+    B.close()
+    for T in transforms:
+        T.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.uneven:
+        run_uneven(a)
     else:
         run_b200(a)
 

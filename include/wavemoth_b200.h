@@ -124,6 +124,13 @@ int wavemoth_plan_lmax(wavemoth_plan plan);
 int64_t wavemoth_plan_device_bytes(wavemoth_plan plan);
 /* Bytes of the compiled butterfly program (interpolants, recurrence data). */
 int64_t wavemoth_plan_program_bytes(wavemoth_plan plan);
+/* Bytes of the plan's device image: the data that does not depend on the
+   number of maps (program, tensor-core and split tables, sliced P and W,
+   ring tables).  Plans made from the same resource file (same path, size
+   and modification time), lmax, mmax and precision flags share one image;
+   it is freed with the last of them.  Included in
+   wavemoth_plan_device_bytes. */
+int64_t wavemoth_plan_image_bytes(wavemoth_plan plan);
 
 /* Caps the device memory a plan may allocate (bytes; <= 0 removes the cap).
    Plans whose buffers would exceed it fail with WAVEMOTH_ERR_NOMEM.  Used to

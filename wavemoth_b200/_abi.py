@@ -35,6 +35,7 @@ SIGNATURES = {
     "wavemoth_plan_lmax": (ctypes.c_int, [_vp]),
     "wavemoth_plan_device_bytes": (ctypes.c_int64, [_vp]),
     "wavemoth_plan_program_bytes": (ctypes.c_int64, [_vp]),
+    "wavemoth_plan_image_bytes": (ctypes.c_int64, [_vp]),
     "wavemoth_set_device_memory_cap": (None, [ctypes.c_int64]),
     "wavemoth_legendre_alm2map_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_plan_timing": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),

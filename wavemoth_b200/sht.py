@@ -113,7 +113,8 @@ class Transform:
                 "split_elems_alm2map": o[8], "split_elems_map2alm": o[9],
                 "split_int8_ops_alm2map": o[10], "split_int8_ops_map2alm": o[11],
                 "device_bytes": _native.lib().wavemoth_plan_device_bytes(self._plan),
-                "program_bytes": _native.lib().wavemoth_plan_program_bytes(self._plan)}
+                "program_bytes": _native.lib().wavemoth_plan_program_bytes(self._plan),
+                "image_bytes": _native.lib().wavemoth_plan_image_bytes(self._plan)}
 
     def close(self):
         if getattr(self, "_plan", None):
