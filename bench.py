@@ -539,8 +539,9 @@ def run_reference(a):
 
 
 def run_uneven(a):
-    """Uneven batch: every request its own plan (nside, 1-8 maps), all
-    alm2map in split precision, captured into one graph by
+    """Uneven batch: every request its own plan (nside, 1-8 maps; plans of
+    one nside share their device image), all alm2map in split precision,
+    captured into one graph by
     wavemoth_b200.batch.Batch; timed against calling the same requests one
     after another on one stream.  Device-resident inputs; L2 is flushed
     between timed launches."""
@@ -559,7 +560,10 @@ def run_uneven(a):
         nmaps = int(rng.integers(1, 9))
         pa = types.SimpleNamespace(nside=nside, lmax=2 * nside, eps=a.eps, chunk=a.chunk, memop=a.memop,
                                    plan_dir=a.plan_dir)
-        T = Transform(ensure_plan(pa, 0), nside, 2 * nside, nmaps, precision="split")
+        # nside 2048 regenerates its residual P at every call: held sliced
+        # (80 GB) it would leave no room for the other requests' images
+        T = Transform(ensure_plan(pa, 0), nside, 2 * nside, nmaps,
+                      precision="split-generate" if nside >= 2048 else "split")
         alm = torch.from_numpy(synthetic_alm(2 * nside, nmaps, 1000 * i)).cuda()
         out = torch.empty((T.npix, nmaps), dtype=torch.float64, device="cuda")
         reqs.append((T, "alm2map", alm, out))
