@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=16,
+                    help="minimum steps of the end-to-end (host buffers) run")
     ap.add_argument("--precision", default="split", choices=["split", "double"],
                     help="split: sliced int8 tensor-core residual products (the plain FP64 path "
                          "is timed beside it and is the error reference); double: plain FP64 only")
@@ -418,19 +420,29 @@ def run_b200(a):
         pipe = HostPipeline(alm.shape, alm.dtype, alm.shape, alm.dtype, e2e_step)
         pipe.run([h_in] * 2, h_out)
         torch.cuda.synchronize()
-        barrier()
-        st = torch.cuda.current_stream()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(st)
-        pipe.run([h_in] * a.steps, [h_out[i & 1] for i in range(a.steps)])
-        f1.record(st)
-        torch.cuda.synchronize()
-        barrier()
-        ems = 1e3 * reduce_max_seconds(f0.elapsed_time(f1) / 1e3, dist if world > 1 else None)
+
+        def e2e_run(n):
+            barrier()
+            st = torch.cuda.current_stream()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(st)
+            pipe.run([h_in] * n, [h_out[i & 1] for i in range(n)])
+            f1.record(st)
+            torch.cuda.synchronize()
+            barrier()
+            return 1e3 * reduce_max_seconds(f0.elapsed_time(f1) / 1e3, dist if world > 1 else None)
+
+        # the first upload and the last download of a run are not overlapped
+        # with a transform; a stream of batches amortises them, so the e2e
+        # value is taken over at least 16 steps (and the K-step figure kept)
+        ek = e2e_run(a.steps)
+        n_e2e = max(a.steps, a.e2e_steps)
+        ems = e2e_run(n_e2e) if n_e2e != a.steps else ek
         nbytes = alm_h.nbytes
-        e2e = {"value": job_rate(world, a.nmaps, a.steps, ems / 1e3), "unit": "maps/s",
+        e2e = {"value": job_rate(world, a.nmaps, n_e2e, ems / 1e3), "unit": "maps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "ms_per_step": ems / a.steps,
+               "ms_per_step": ems / n_e2e, "steps": n_e2e,
+               "value_at_k_steps": job_rate(world, a.nmaps, a.steps, ek / 1e3),
                "api": "wavemoth_b200.pipeline.HostPipeline over Transform.alm2map/map2alm "
                       "(uploads and downloads overlapped with the neighbouring steps' transforms)"}
         del pipe
