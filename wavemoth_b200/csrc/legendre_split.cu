@@ -67,7 +67,7 @@ constexpr int kSliceA = kSplitM * kSplitK;                    // 8192 bytes
 constexpr int kSliceB = kSplitN * kSplitK;                    // 4096
 constexpr int kStageA = kSplitSlices * kSliceA;               // 49152
 constexpr int kStageB = kSplitPlane;                          // 24576
-constexpr int kXsStride = kSplitN + 2;                        // epilogue tile row (doubles)
+constexpr int kXsStride = kSplitN + 1;  // epilogue tile row (doubles); odd: row-per-lane stores are free of bank conflicts
 constexpr long long kWaitLimit = 1LL << 26;
 static_assert(kSplitDiag * 64 <= kTmemCols, "diagonal accumulators exceed TMEM");
 static_assert(kSplitM * kXsStride * 8 <= 2 * kStageA, "epilogue tile exceeds the A stages");
