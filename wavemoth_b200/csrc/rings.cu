@@ -399,8 +399,8 @@ __device__ __forceinline__ bool lane_live(const RingCta &c, int g, int side) {
 }
 
 // q values (even part a, odd part b) of the first term of the aliasing sums
-// of bin j, m = j (zero when j > mmax).  Loaded for a batch of bins before
-// any is summed, so that a thread has its q loads in flight together.
+// of bin j, m = j (zero when j > mmax).  Loaded one item ahead of the sums,
+// so that a thread's next q loads are in flight while it sums.
 __device__ __forceinline__ void first_term(const double *qg, int j, int mmax, int64_t qstride, int64_t half,
                                            bool live, cplx &a, cplx &b) {
   if (live && j <= mmax) {
@@ -438,8 +438,6 @@ __device__ __forceinline__ void alias_sums(const double *qg, int j, int n, int m
   }
 }
 
-constexpr int kGatherBatch = 2;  // bins per thread whose first q loads are issued together (2 measured best)
-
 __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p) {
   extern __shared__ double smem_d[];
   const RingCta c = ring_cta(p, blockIdx.x);
@@ -461,27 +459,27 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
     // Z[k] and Z[N - k] (natural order, chirped for Bluestein rings) of the
     // CTA's hemispheres, from W[k] and W[N - k]
     const int npairs = (N >> 1) + 1, nitems = npairs << c.lgm;
-    for (int t0 = threadIdx.x; t0 < nitems; t0 += kGatherBatch * blockDim.x) {
-      cplx qa[kGatherBatch][2], qb[kGatherBatch][2];  // first-term q at kk and N - kk
-#pragma unroll
-      for (int u = 0; u < kGatherBatch; ++u) {
-        const int t = t0 + u * blockDim.x;
-        const int mi = t & gmm, kk = t >> c.lgm;
-        const bool live = t < nitems && mi < c.nm;
-        const double *qg = qbase + 2 * mi;
-        first_term(qg, kk, p.mmax, qstride, half, live, qa[u][0], qb[u][0]);
-        first_term(qg, N - kk, p.mmax, qstride, half, live && N - kk != kk, qa[u][1], qb[u][1]);
-      }
-#pragma unroll
-      for (int u = 0; u < kGatherBatch; ++u) {
-        const int t = t0 + u * blockDim.x;
-        if (t >= nitems) break;
+    // software pipeline over this thread's items: the first-term q of item
+    // t + blockDim is in flight while item t is summed
+    auto fetch = [&](int t, cplx (&qa)[2], cplx (&qb)[2]) {
+      const int mi = t & gmm, kk = t >> c.lgm;
+      const bool live = t < nitems && mi < c.nm;
+      const double *qg = qbase + 2 * mi;
+      first_term(qg, kk, p.mmax, qstride, half, live, qa[0], qb[0]);
+      first_term(qg, N - kk, p.mmax, qstride, half, live && N - kk != kk, qa[1], qb[1]);
+    };
+    cplx qa[2], qb[2];
+    fetch(threadIdx.x, qa, qb);
+    for (int t = threadIdx.x; t < nitems; t += blockDim.x) {
+      cplx na[2], nb[2];
+      fetch(t + blockDim.x, na, nb);
+      {
         const int mi = t & gmm, kk = t >> c.lgm, kr = N - kk;
         cplx Aa = {0.0, 0.0}, Ba = {0.0, 0.0}, Ab = {0.0, 0.0}, Bb = {0.0, 0.0};  // at kk and N - kk
         if (mi < c.nm) {
           const double *qg = qbase + 2 * mi;
-          alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, qa[u][0], qb[u][0], Aa, Ba);
-          if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, qa[u][1], qb[u][1], Ab, Bb);
+          alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, qa[0], qb[0], Aa, Ba);
+          if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, qa[1], qb[1], Ab, Bb);
           else { Ab = Aa; Bb = Ba; }
         }
 #pragma unroll
@@ -506,6 +504,10 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
           }
         }
       }
+      qa[0] = na[0];
+      qa[1] = na[1];
+      qb[0] = nb[0];
+      qb[1] = nb[1];
     }
     if (!c.pow2)
       for (int t = threadIdx.x; t < ((M - N) << lg); t += blockDim.x)
