@@ -179,3 +179,42 @@ def test_config1_nside64_against_reference():
     else:
         want = osht.alm2map_butterfly(osht.Rev1File(path), alm, lmax)
     assert rel(got, want) < 1e-10
+
+
+def test_config2_nside512_round_trip():
+    """Round trip alm2map -> map2alm at nside 512, lmax 1024, 1 map, alm
+    re/im ~ N(0,1)(l+1)^-1.5, plan ID eps 1e-12: alm2map within 1e-10 of the
+    reference's own C transform (or the oracle's butterfly), map2alm pinned
+    to it through the adjoint identity at this size, and the split path's
+    map and round trip within 1e-9 of the FP64 ones."""
+    import os
+    ref = pytest.importorskip("oracle.ref")
+    nside, lmax = 512, 1024
+    npix = 12 * nside * nside
+    path = plan_file(nside, lmax, 64, 1e-12, 20.0, workers=min(os.cpu_count() or 1, 32))
+    alm = osht.random_alm(lmax, 1, seed=2, power=1.5)
+    maps, _ = _alm2map_gpu(path, nside, lmax, alm)
+    if ref.available():
+        rp = ref.RefPlan(nside, lmax, 1, path, nthreads=8)
+        rp.input[:] = alm
+        want = rp.execute().copy()
+        rp.close()
+        assert rel(maps, want) < 1e-10
+    back = _map2alm_gpu(path, nside, lmax, maps)
+    f = np.random.default_rng(3).standard_normal((npix, 1))
+    b = _map2alm_gpu(path, nside, lmax, f)
+    lhs = float(np.sum(maps * f))
+    rhs = osht.weighted_alm_dot(alm, b, lmax) * npix / (4 * np.pi)
+    assert abs(lhs - rhs) <= 1e-11 * (abs(lhs) + np.linalg.norm(maps) * np.linalg.norm(f))
+    out = np.zeros((npix, 1))
+    p = wlib.ShtPlan(nside, lmax, lmax, np.ascontiguousarray(alm), out, "mmajor", matrix_data_filename=path,
+                     precision="split")
+    maps_s = p.execute().copy()
+    p.close()
+    alm_s = np.zeros_like(alm)
+    p = wlib.ShtPlan(nside, lmax, lmax, np.ascontiguousarray(maps_s), alm_s, "mmajor",
+                     matrix_data_filename=path, direction="map2alm", precision="split")
+    back_s = p.execute().copy()
+    p.close()
+    assert np.abs(maps_s - maps).max() <= 1e-9 * np.abs(maps).max()
+    assert np.abs(back_s - back).max() <= 1e-9 * np.abs(back).max()
