@@ -144,6 +144,12 @@ void wavemoth_set_device_memory_cap(int64_t bytes);
    for the recorded events. */
 int wavemoth_plan_timing(wavemoth_plan plan, int mode, double *out);
 
+/* Test hook: one_side = 1 makes the ring kernels run the two hemispheres of
+   every ring pair one after the other within a CTA (the layout used for
+   transforms longer than 4096 points, nside 2048), 0 restores the default
+   (both hemispheres at once where they fit).  Results are the same. */
+int wavemoth_plan_set_hemisphere_mode(wavemoth_plan plan, int one_side);
+
 /* Number of this library's kernels launched by the plan's executes since the
    last wavemoth_plan_timing reset (mode 0 or 1); -1 for a NULL plan. */
 int64_t wavemoth_plan_kernel_launches(wavemoth_plan plan);

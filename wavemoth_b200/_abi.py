@@ -40,6 +40,7 @@ SIGNATURES = {
     "wavemoth_legendre_alm2map_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_plan_timing": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "wavemoth_plan_kernel_launches": (ctypes.c_int64, [_vp]),
+    "wavemoth_plan_set_hemisphere_mode": (ctypes.c_int, [_vp, ctypes.c_int]),
     "wavemoth_plan_work": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "wavemoth_check_resourcefile": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                                    ctypes.POINTER(ctypes.c_int64)]),
