@@ -163,7 +163,7 @@ def test_dot_product_adjoint(cfg):
 
 
 def test_config1_nside64_against_reference():
-    """BASELINE config: plain FP64 alm2map, nside 64, lmax 128, 1 map,
+    """Headline configuration 1: plain FP64 alm2map, nside 64, lmax 128, 1 map,
     re/im ~ N(0,1)(l+1)^-1 seeded, plan eps 1e-10 chunk 64: <= 1e-10
     relative to the reference's own FP64 transform."""
     ref = pytest.importorskip("oracle.ref")

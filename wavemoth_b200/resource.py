@@ -16,7 +16,7 @@ wavemoth/butterfly.pyx:527-825, scripts/precompute.py), restated:
   (lib.pyx:397-486 with stripify at :301-368), each strip holding x^2 and the
   two starting rows; blocks of at most 4 rows are stored dense.
 * the binary layout is rev1 (src/wavemoth.c:203-264, src/butterfly.c.in:
-  434-445, src/butterfly.h.in:8-88): see DESIGN.md.
+  434-445, src/butterfly.h.in:8-88), byte for byte.
 
 Differences from the reference writer that do not change the format:
 the ID is this library's own pivoted-QR implementation (wm_host_interp_decomp,
