@@ -59,9 +59,9 @@ def parse():
                          "graph launch, against the same requests called one after another")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--uneven-nsides", default="64,128,256,512")
-    ap.add_argument("--check", action="store_true",
-                    help="also report the round-trip relative error of map 0 vs the FP64 oracle "
-                         "at a reduced size (slow on CPU)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the comparison of maps 0-3 with the reference's own C alm2map "
+                         "(run outside the timed region, rank 0 at N = 1)")
     a = ap.parse_args()
     if a.lmax is None:
         a.lmax = 2 * a.nside
@@ -222,8 +222,8 @@ class ReferenceRunner:
         self.rp.close()
 
 
-def reference_rate(a, path, seconds):
-    r = ReferenceRunner(a, path)
+def reference_rate(a, path, seconds, runner=None):
+    r = runner if runner is not None else ReferenceRunner(a, path)
     r.execute()  # warm-up: page-in and first touch
     times = []
     t_end = time.time() + seconds
@@ -308,6 +308,41 @@ def profile_traffic(kernel):
     return None
 
 
+def adjoint_identity(torch, T, alm, maps, npix, seed=7):
+    """map2alm pinned through the adjoint identity on every map of the batch:
+    <alm2map(a), f> = (npix / 4 pi) sum_lm c_m Re(a_lm conj(map2alm(f)_lm))
+    (c_0 = 1, c_m = 2) for a seeded Gaussian map f; returns the largest
+    |lhs - rhs| / (|alm2map(a)| |f|) over the maps."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    f = torch.randn(maps.shape, dtype=torch.float64, device="cuda", generator=g)
+    b = T.map2alm(f)
+    lmax = T.lmax
+    w = torch.cat([torch.full((lmax - m + 1,), 1.0 if m == 0 else 2.0, dtype=torch.float64)
+                   for m in range(lmax + 1)]).cuda()
+    lhs = (maps * f).sum(0)
+    rhs = (w[:, None] * (alm * b.conj()).real).sum(0) * (npix / (4 * np.pi))
+    den = maps.norm(dim=0) * f.norm(dim=0)
+    return float(((lhs - rhs).abs() / den).max())
+
+
+def headline_parity(runner, head, nmaps):
+    """Maps 0-3 of the GPU batch against the reference's own alm2map of the
+    same seeded alm: max |gpu - ref| / max |ref| and the relative L2 error."""
+    ref = runner.rp.execute().copy()
+    k = min(ref.shape[1], nmaps)
+    out = {"reference": "reference C wavemoth_execute (oracle/_ref) on the same plan file, maps 0-%d"
+                        % (k - 1)}
+    for name in ("plain", "double", "split"):
+        if name not in head:
+            continue
+        got = head[name][:, :k]
+        key = "plain" if name == "double" else name
+        out[key] = {"max_rel_error_map": float(np.abs(got - ref[:, :k]).max() / np.abs(ref[:, :k]).max()),
+                    "rel_l2_error_map": float(np.linalg.norm(got - ref[:, :k]) / np.linalg.norm(ref[:, :k]))}
+    return out
+
+
 def run_b200(a):
     import torch
     import torch.distributed as dist
@@ -342,6 +377,7 @@ def run_b200(a):
 
     # plain FP64 path beside the split one: its rate and the split error
     plain = None
+    head = {}  # maps 0-3 of both paths, compared with the reference after the timed region
     if a.precision == "split":
         TP = Transform(path, a.nside, a.lmax, a.nmaps, precision="double")
         maps_p = torch.empty_like(maps)
@@ -375,6 +411,9 @@ def run_b200(a):
                  "max_rel_error_alm_round_trip": maxrel(alm_out, alm_p),
                  "error_definition": "max |split - plain FP64| / max |plain FP64| over the alm2map "
                                      "output and over the alm2map+map2alm output, same inputs"}
+        head["plain"] = maps_p[:, :4].cpu().numpy()
+        head["adjoint"] = {"plain": adjoint_identity(torch, TP, alm, maps_p, T.npix),
+                           "split": adjoint_identity(torch, T, alm, maps, T.npix)}
         TP.close()
         del maps_p, alm_p
 
@@ -402,6 +441,7 @@ def run_b200(a):
     ms = 1e3 * reduce_max_seconds(ms / 1e3, dist if world > 1 else None)
     ms_per_step = ms / a.steps
     value = job_rate(world, a.nmaps, a.steps, ms / 1e3)
+    head[a.precision] = maps[:, :4].cpu().numpy()  # every step recomputes maps from the same alm
 
     # ---------------- end to end (host buffers) ----------------
     # every step uploads its alm from pinned host memory and downloads its
@@ -486,13 +526,29 @@ def run_b200(a):
     roofline["kernel_ms_per_launch"] = kms
     roofline["kernel_time_share"] = share
 
-    # ---------------- CPU baseline (rank 0, N = 1) ----------------
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    # ---------------- parity and CPU baseline (rank 0, N = 1) ----------------
+    # maps 0-3 of the batch (seeds 1000-1003) against the reference's own C
+    # alm2map of the same alm on the same plan file; the same runner is then
+    # timed as the CPU baseline
+    cpu, parity, runner = None, None, None
+    if rank == 0 and world == 1 and not (a.no_cpu_baseline and a.no_parity):
         try:
-            cpu = reference_rate(a, path, a.cpu_baseline_seconds)
+            runner = ReferenceRunner(a, path)
         except Exception as ex:  # reported, never fatal for the GPU number
+            err = str(ex)[:200]
+            parity = {"unavailable": "reference C library: " + err}
+            cpu = {"value": None, "unit": "maps/s", "error": err}
+    if runner is not None and not a.no_parity:
+        parity = headline_parity(runner, head, a.nmaps)
+    if runner is not None and not a.no_cpu_baseline:
+        try:
+            cpu = reference_rate(a, path, a.cpu_baseline_seconds, runner=runner)
+        except Exception as ex:
             cpu = {"value": None, "unit": "maps/s", "error": str(ex)[:200]}
+    elif runner is not None:
+        runner.close()
+    if parity is not None and "adjoint" in head:
+        parity["adjoint_identity"] = head["adjoint"]
 
     launches = kt["kernels"]  # this library's kernels launched in the timed steps
     out = {
@@ -507,6 +563,7 @@ def run_b200(a):
                                  "products i+j<=6), FP64 recurrence/levels/rings"
                                  if a.precision == "split" else "plain FP64"),
                    "plain_fp64": plain,
+                   "parity_vs_reference": parity,
                    "plan": {"eps": a.eps, "chunk": a.chunk,
                                                        "memop_cost": a.memop},
                    "parallelism": "replicas (maps sharded per GPU)" if world > 1 else "1 GPU",

@@ -103,11 +103,15 @@ void wavemoth_batch_destroy(wavemoth_batch batch);
    until the process exits; nothing is allocated or freed by this call.
    Problems whose per-CTA buffers (2 x largest level x 2 nmaps doubles) do
    not fit are rejected with WAVEMOTH_ERR_NOMEM; smaller ones run on as many
-   CTAs as fit.  The first call on a device looks up the array's device
-   address (cudaGetSymbolAddress), so make it before any stream capture.
-   All calls share the array and its contents persist between calls: calls
-   that overlap on the GPU race, so serialise them.  No counterpart in the
-   reference. */
+   CTAs as fit.  The array's device address is looked up
+   (cudaGetSymbolAddress) when a plan is created on a device, which loads
+   the module holding the array: the 32 MiB are taken then, together with
+   the code of the kernel this call launches, so the call itself makes the
+   driver allocate nothing.  The kernel is the generic FP64 butterfly kernel
+   over every (m, parity) matrix, so q agrees with the plan's own path to
+   rounding.  All calls share the array and its contents persist between
+   calls: calls that overlap on the GPU race, so serialise them.  No
+   counterpart in the reference. */
 int wavemoth_legendre_alm2map_noalloc(wavemoth_plan plan, const double *alm, double *q,
                                       void *stream);
 
@@ -136,6 +140,18 @@ int64_t wavemoth_plan_image_bytes(wavemoth_plan plan);
    Plans whose buffers would exceed it fail with WAVEMOTH_ERR_NOMEM.  Used to
    exercise allocation-failure handling without exhausting the GPU. */
 void wavemoth_set_device_memory_cap(int64_t bytes);
+
+/* Test hook: how many times a wait of the streamed split-precision GEMM
+   (wavemoth_execute_*_device with WAVEMOTH_PRECISION_SPLIT) polls its
+   mbarrier for another warp role before it gives up (0 restores the
+   default, about a second).  A wait that gives up records a timeout in the
+   plan's device status word, which wavemoth_plan_device_status reports as
+   WAVEMOTH_ERR_DEVICE; the kernel then
+   waits for the copies and MMAs it already issued, frees its tensor memory
+   and returns, so the context stays usable.  With a tiny limit a call
+   fails this way on purpose.  New; it replaces the reference's abort() on a
+   failed check (src/wavemoth_error.h:1-19). */
+int wavemoth_plan_set_wait_limit(wavemoth_plan plan, int64_t polls);
 
 /* Per-kernel device timing of a plan, from CUDA events recorded on the
    launching stream.  mode 1: reset and enable, 0: reset and disable,

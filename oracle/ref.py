@@ -20,15 +20,21 @@ MAX_THREADS = 8
 
 
 def available():
-    return os.path.exists(REF_LIB) or os.path.isdir(os.environ.get("WAVEMOTH_REFERENCE",
-                                                                    "/root/reference"))
+    """The reference library is built, or can be built from the checkout
+    named by WAVEMOTH_REFERENCE."""
+    ref = os.environ.get("WAVEMOTH_REFERENCE")
+    return os.path.exists(REF_LIB) or bool(ref and os.path.isdir(os.path.join(ref, "src")))
 
 
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(REF_LIB):
-            ref = os.environ.get("WAVEMOTH_REFERENCE", "/root/reference")
+            ref = os.environ.get("WAVEMOTH_REFERENCE")
+            if not ref:
+                raise RuntimeError("oracle/_ref/libwavemoth_ref.so is not built; run "
+                                   "make -C oracle ref REF=<reference checkout> or set "
+                                   "WAVEMOTH_REFERENCE")
             subprocess.run(["make", "-C", _HERE, "ref", "REF=" + ref], check=True,
                            capture_output=True)
         L = ctypes.CDLL(REF_LIB)

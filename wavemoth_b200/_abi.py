@@ -37,6 +37,7 @@ SIGNATURES = {
     "wavemoth_plan_program_bytes": (ctypes.c_int64, [_vp]),
     "wavemoth_plan_image_bytes": (ctypes.c_int64, [_vp]),
     "wavemoth_set_device_memory_cap": (None, [ctypes.c_int64]),
+    "wavemoth_plan_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_int64]),
     "wavemoth_legendre_alm2map_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_plan_timing": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "wavemoth_plan_kernel_launches": (ctypes.c_int64, [_vp]),

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "plan.h"
 
 namespace wm {
@@ -86,6 +88,7 @@ struct SplitParams {
   double *q;                      // alm2map: q
   double *xbuf;
   int32_t *status;                // device status word (kStatus*)
+  int64_t wait_limit;             // polls of a streamed-GEMM wait for another role (0: default)
   // level products of depth-1 roots
   const DevPair *pairs;
   const int32_t *i32;
@@ -121,11 +124,18 @@ cudaError_t launch_residual_slices(const SplitParams &prm, const StreamLaunch &a
 //        4 alm2map level operand (X) slices, 6 map2alm level operand (q~) slices;
 // the level GEMMs and the residual GEMMs on sliced P run as launch_stream.
 cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream_t st);
+// Zeroes vectors [v0, v0 + kSplitN) of the rows listed in `rows` (n entries,
+// (buffer << kZeroBufShift) | row with buffer 0 q, 1 X buffer, 2 alm).
+cudaError_t launch_zero_rows(const SplitParams &prm, const int64_t *rows, int32_t n, cudaStream_t st);
 // Plan creation: P scales of both directions, and the sliced W of the levels.
 cudaError_t launch_split_scales(const SplitParams &prm, cudaStream_t st);
 cudaError_t launch_level_slices(const SplitParams &prm, cudaStream_t st);
 
 int legendre_threads();
+cudaError_t legendre_preload();
+// Device address and size of the allocation-free entry point's static
+// scratch array on the current device (noalloc.cu); 0 on success.
+int noalloc_scratch(void **out, size_t *bytes, std::string &err);
 cudaError_t launch_legendre(bool alm2map, const LegendreParams &prm, int grid, cudaStream_t st);
 
 struct RingParams {

@@ -318,6 +318,17 @@ cudaError_t launch_vc(bool forward, const LegendreParams &prm, int grid, cudaStr
 
 int legendre_threads() { return kThreads; }
 
+// Loads the alm2map kernels' module now (module loading is lazy by default:
+// the first launch would otherwise load it, and loading allocates device
+// memory for the code).
+cudaError_t legendre_preload() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k_alm2map_legendre<2>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_alm2map_legendre<4>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_alm2map_legendre<8>);
+  return e;
+}
+
 cudaError_t launch_legendre(bool alm2map, const LegendreParams &prm, int grid, cudaStream_t st) {
   if (prm.nvecs <= 2) return launch_vc<2>(alm2map, prm, grid, st);
   if (prm.nvecs <= 4) return launch_vc<4>(alm2map, prm, grid, st);

@@ -51,6 +51,8 @@
 // bounded: on expiry the kernel records kStatusTimeout, stops issuing work,
 // waits (bounded) for its MMAs and copies, frees its TMEM and returns.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "kernels.h"
@@ -362,6 +364,20 @@ __global__ void __launch_bounds__(256) k_split_operand_x(SplitParams p) {
   for (int gi = blockIdx.x; gi < p.ngroups; gi += gridDim.x) {
     slice_operand<1>(p, gi);
     __syncthreads();
+  }
+}
+
+// One warp per listed row: vectors [v0, v0 + kSplitN) of the row set to zero.
+__global__ void __launch_bounds__(256) k_zero_rows(SplitParams p, const int64_t *rows, int32_t n) {
+  const int vn = min(kSplitN, p.nvecs - p.v0);
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+       i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t e = rows[i];
+    const int buf = (int)(e >> kZeroBufShift);
+    const int64_t row = e & ((1LL << kZeroBufShift) - 1);
+    double *dst = (buf == 0 ? p.q : buf == 1 ? p.xbuf : p.alm_out) + row * p.nvecs + p.v0;
+    for (int v = lane; v < vn; v += 32) dst[v] = 0.0;
   }
 }
 
@@ -841,10 +857,14 @@ struct StreamSmem {
   int32_t abort;
 };
 
-// Bounded wait that also ends when *abort is set; false unless completed.
-__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t phase, volatile int32_t *abort) {
+// Bounded wait (at most `limit` polls) that also ends when *abort is set;
+// false unless completed.  The waits for progress of another role use the
+// plan's limit; the drains before exit keep kWaitLimit (copies and MMAs
+// already issued always complete in hardware).
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t phase, volatile int32_t *abort,
+                                                   long long limit) {
   uint32_t done = 0;
-  for (long long it = 0; it < kWaitLimit; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
@@ -900,6 +920,7 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
   int32_t *erow = reinterpret_cast<int32_t *>(evs + kSplitN);  // destination row of each tile row
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile int32_t *abort = &ss->abort;
+  const long long lim = p.wait_limit > 0 ? p.wait_limit : kWaitLimit;
   if (warp == 0) tmem_alloc(&ss->tmem);
   if (tid == 0) {
     for (int s = 0; s < kStreamStages; ++s) {
@@ -928,7 +949,7 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
         for (int c = 0; c < T.nk; ++c, ++g) {
           const int s = (int)(g % kStreamStages);
           const long long use = g / kStreamStages;
-          if (use > 0 && !mbar_wait_or_abort(&ss->empty[s], (uint32_t)((use - 1) & 1), abort)) break;
+          if (use > 0 && !mbar_wait_or_abort(&ss->empty[s], (uint32_t)((use - 1) & 1), abort, lim)) break;
           const uint32_t dst = smem_u32(smem + s * kStreamStage);
           expect_tx(&ss->full[s], kStreamStage);
           bulk_load(dst, L.a + (T.a + c) * (int64_t)kStageA, kStageA, &ss->full[s]);
@@ -949,12 +970,12 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
       int nt = 0;
       for (int t = blockIdx.x; t < L.ntiles && !*abort; t += gridDim.x, ++nt) {
         const DevStreamTile T = L.tiles[t];
-        if (nt > 0 && !mbar_wait_or_abort(&ss->acc_empty, (uint32_t)((nt - 1) & 1), abort)) break;
+        if (nt > 0 && !mbar_wait_or_abort(&ss->acc_empty, (uint32_t)((nt - 1) & 1), abort, lim)) break;
         fence_after_sync();
         bool ok = true;
         for (int c = 0; c < T.nk; ++c, ++g) {
           const int s = (int)(g % kStreamStages);
-          if (!mbar_wait_or_abort(&ss->full[s], (uint32_t)((g / kStreamStages) & 1), abort)) {
+          if (!mbar_wait_or_abort(&ss->full[s], (uint32_t)((g / kStreamStages) & 1), abort, lim)) {
             ok = false;
             break;
           }
@@ -994,7 +1015,7 @@ __global__ void __launch_bounds__(kStreamThr, 1) k_stream_split(SplitParams p, S
       } else if (etid < kSplitM + kSplitN) {
         evs[etid - kSplitM] = p.vec_scale[(int64_t)T.vs * kSplitN + etid - kSplitM].y;
       }
-      const bool ok = mbar_wait_or_abort(&ss->acc_full, (uint32_t)(nt & 1), abort);
+      const bool ok = mbar_wait_or_abort(&ss->acc_full, (uint32_t)(nt & 1), abort, lim);
       if (epi_sync_or(!ok || *abort)) break;
       fence_after_sync();
       const double rinv = erinv[row];
@@ -1159,6 +1180,13 @@ cudaError_t launch_split(int which, const SplitParams &prm, int grid, cudaStream
     default:
       return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zero_rows(const SplitParams &prm, const int64_t *rows, int32_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int grid = (int)std::min<int64_t>(((int64_t)n + 7) / 8, 4096);
+  k_zero_rows<<<grid, 256, 0, st>>>(prm, rows, n);
   return cudaGetLastError();
 }
 

@@ -4,17 +4,24 @@
 // code inside a custom allocator's callback, a process whose memory is
 // managed by a framework that forbids outside allocations, or a step that
 // must not trigger driver allocations while other work is latency
-// critical.  wavemoth_legendre_alm2map_noalloc runs the same butterfly
-// Legendre kernel as the plan's own path, but takes its per-CTA level
-// buffers and its work-queue counter from the file-scope device array below
-// instead of plan-allocated scratch.  The caller passes the input (alm) and
-// the output (q) as device pointers; the plan (created beforehand) supplies
-// the compiled butterfly program.
+// critical.  wavemoth_legendre_alm2map_noalloc runs the generic FP64
+// butterfly Legendre kernel (k_alm2map_legendre, SIMT, persistent CTAs on a
+// work queue) over every (m, parity) matrix of the plan; the plan's own path
+// runs that kernel only for trees of depth >= 2 and the FP64 tensor-core
+// kernels for the rest, so the two agree to rounding, not bitwise.  Its
+// per-CTA level buffers and its work-queue counter come from the
+// file-scope device array below instead of plan-allocated scratch.  The
+// caller passes the input (alm) and the output (q) as device pointers; the
+// plan (created beforehand) supplies the compiled butterfly program.
 //
 // The array is a fixed 32 MiB that every GPU which loads the library holds
-// until the process exits.  All calls share it, so calls that overlap on the
-// GPU (on different streams, or from different host threads) race on it;
-// serialise them.  The counter at its start is cleared on every call.
+// until the process exits.  Its device address is resolved when a plan is
+// created on a device (abi.cpp), which loads the module holding it: that is
+// when the 32 MiB are taken, and the kernel's module is loaded then too, so
+// the call itself makes the driver allocate nothing.  All calls share the
+// array, so calls that overlap on the GPU (on different streams, or from
+// different host threads) race on it; serialise them.  The counter at its
+// start is cleared on every call.
 #include <cuda_runtime.h>
 #include <stdint.h>
 

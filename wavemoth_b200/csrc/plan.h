@@ -161,6 +161,10 @@ struct DevSplitRoot {
   int32_t nzc, nsc;         // chunks of 64 over z and over s
 };
 
+// Rows that no split tile writes, zeroed before the launch they belong to:
+// (buffer << kZeroBufShift) | row, buffer 0 q, 1 X buffer, 2 alm.
+constexpr int kZeroBufShift = 56;
+
 struct DevSplitLevelTile {  // <= kSplitM rows (z or s) of one root unit
   int32_t unit, row0, nrows, pad;
 };

@@ -528,6 +528,11 @@ static void build_split_tables(HostProgram &P) {
   int64_t apl = 0, xpl = 0, rows = 0;
   std::vector<std::pair<int32_t, DevSplitTileA>> ta;
   std::vector<std::pair<int32_t, DevSplitTileB>> tb;
+  for (auto &z : P.split_zero) z.clear();
+  const int64_t ni = 2 * (int64_t)P.nside;
+  auto zero = [&](int launch, int64_t buf, int64_t row) {
+    P.split_zero[launch].push_back((buf << kZeroBufShift) | row);
+  };
   for (int32_t gi = 0; gi < (int32_t)P.groups.size(); ++gi) {
     const DevGroup &G = P.groups[gi];
     DevSplitGroup S{};
@@ -545,11 +550,25 @@ static void build_split_tables(HostProgram &P) {
       for (int32_t c = c0; c < c0 + T.ncols; ++c)
         T.kc0 = std::min(T.kc0, P.gcols[G.cols + c].start);
       T.kc0 /= kSplitK;
-      if (T.kc0 < S.nrchunks) ta.push_back({S.nrchunks - T.kc0, T});
+      if (T.kc0 < S.nrchunks) {
+        ta.push_back({S.nrchunks - T.kc0, T});
+      } else {
+        // no active row in any column of the tile: its outputs are zero
+        const DevMatrix &M = P.mats[G.matrix];
+        const int64_t base = G.in_q ? (int64_t)(2 * M.m + M.odd) * ni : (int64_t)M.xrow;
+        for (int32_t c = c0; c < c0 + T.ncols; ++c)
+          zero(kStreamResA2M, G.in_q ? 0 : 1, base + P.gcols[G.cols + c].row);
+      }
     }
-    if (S.ncchunks > 0)
+    if (S.ncchunks > 0) {
       for (int32_t r0 = 0; r0 < G.nrows; r0 += kSplitM)
         tb.push_back({S.ncchunks, DevSplitTileB{gi, r0, std::min(kSplitM, G.nrows - r0), 0}});
+    } else {
+      // no skeleton column: the group's alm rows are zero
+      const DevMatrix &M = P.mats[G.matrix];
+      const int64_t arow0 = (int64_t)M.m * (2 * P.lmax - M.m + 3) / 2 + M.odd;
+      for (int32_t r = 0; r < G.nrows; ++r) zero(kStreamResM2A, 2, arow0 + 2 * (int64_t)(G.rs + r));
+    }
   }
   std::stable_sort(ta.begin(), ta.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
   std::stable_sort(tb.begin(), tb.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
@@ -583,9 +602,14 @@ static void build_split_tables(HostProgram &P) {
     R.rs_m2a = lrows;
     lrows += K;
     P.sroots.push_back(R);
-    if (R.nsc > 0)
+    if (R.nsc > 0) {
       for (int32_t z0 = 0; z0 < pr.n; z0 += kSplitM)
         la.push_back({R.nsc, DevSplitLevelTile{u, z0, std::min(kSplitM, pr.n - z0), 0}});
+    } else {
+      // a root without skeleton rows: its q rows are zero
+      const DevMatrix &M = P.mats[P.roots[u].matrix];
+      for (int32_t z = 0; z < pr.n; ++z) zero(kStreamLevelA2M, 0, (int64_t)(2 * M.m + M.odd) * ni + pr.out_left + z);
+    }
     if (R.nzc > 0)
       for (int32_t s0 = 0; s0 < K; s0 += kSplitM)
         lm.push_back({R.nzc, DevSplitLevelTile{u, s0, std::min(kSplitM, K - s0), 0}});

@@ -45,6 +45,11 @@ struct HostProgram {
   std::vector<DevStreamTile> stream_tiles[4];
   std::vector<int32_t> stream_rows[4], stream_sidx[4];
   int64_t stream_res_achunks = 0;       // A chunks of sliced residual P, both directions
+  // destination rows that no split tile writes (columns with no active row,
+  // roots with no skeleton) and that must read as zero, per launch
+  // (kStream* order); encoded kZeroBufShift-bit buffer (0 q, 1 X, 2 alm)
+  // above the row index
+  std::vector<int64_t> split_zero[4];
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)
