@@ -24,8 +24,10 @@ struct LegendreParams {
   int32_t ni;             // rings per hemisphere incl. equator (2 * nside)
   const double *alm_in;   // alm2map: (nalm, nvecs)
   double *alm_out;        // map2alm: (nalm, nvecs)
-  const double *q_in;     // map2alm: (2(mmax+1), ni, nvecs)
-  double *q_out;          // alm2map
+  const double *q_in;     // map2alm: q~ (q layout: row of (m, parity, ring) at
+                          // (2m + parity) q_mstride + ring q_rstride doubles)
+  double *q_out;          // alm2map: q
+  int64_t q_mstride, q_rstride;
   double *scratch;        // gridDim.x slots of slot_stride doubles
   int64_t slot_stride;    // 2 * max_rows * nvecs
   int32_t *counter;       // work queue head (zeroed before launch)
@@ -52,6 +54,7 @@ struct FastParams {
   double *alm_out;         // map2alm output
   const double *q_in;      // map2alm input q~
   double *q;               // alm2map output q
+  int64_t q_mstride, q_rstride;  // q row of (m, parity, ring): (2m + parity) q_mstride + ring q_rstride
   double *xbuf;            // depth-1 root blocks: X buffer (xrows x nvecs)
 };
 
@@ -86,6 +89,7 @@ struct SplitParams {
   double *alm_out;
   const double *q_in;             // map2alm: q~
   double *q;                      // alm2map: q
+  int64_t q_mstride, q_rstride;   // q row of (m, parity, ring): (2m + parity) q_mstride + ring q_rstride
   double *xbuf;
   int32_t *status;                // device status word (kStatus*)
   int64_t wait_limit;             // polls of a streamed-GEMM wait for another role (0: default)
@@ -145,7 +149,7 @@ struct RingParams {
   int32_t mmax;
   int32_t nmaps;
   int32_t nvecs;
-  const double *q;        // synthesis input (2(mmax+1), ni, nvecs)
+  const double *q;        // synthesis input: rows of nvecs doubles, (m, parity) of ring r at (r (mmax + 1) + m) 2 + parity
   double *map;            // synthesis output (npix, nmaps)
   const double *map_in;   // analysis input (npix, nmaps)
   double *q_out;          // analysis output

@@ -66,8 +66,9 @@ __global__ void __launch_bounds__(kThreads) k_alm2map_legendre(LegendreParams p)
     int idx = next_matrix(p.counter, &s_idx);
     if (idx >= p.nmats) break;
     const DevMatrix M = p.mats[p.order[idx]];
-    double *qm = p.q_out + (int64_t)(2 * M.m + M.odd) * p.ni * nvecs;
+    double *qm = p.q_out + (int64_t)(2 * M.m + M.odd) * p.q_mstride;
     double *level0 = M.nlevels > 0 ? A : qm;
+    const int64_t l0s = M.nlevels > 0 ? nvecs : p.q_rstride;  // row stride of level0
     const int64_t arow0 = alm_row0(M, p.lmax);
 
     // ---- residual stage: one item per (depth-0 row, vector chunk) ----
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(kThreads) k_alm2map_legendre(LegendreParams p)
           for (int v = 0; v < VC; ++v) acc[v] += nv2 * x[v];
         }
       }
-      double *out = level0 + (int64_t)row * nvecs + v0;
+      double *out = level0 + (int64_t)row * l0s + v0;
 #pragma unroll
       for (int v = 0; v < VC; ++v)
         if (v < nv) out[v] = acc[v];
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(kThreads) k_alm2map_legendre(LegendreParams p)
       const DevLevel L = p.levels[M.level_begin + t];
       const double *upper = (t & 1) ? B : A;
       double *lower = (t == M.nlevels - 1) ? qm : ((t & 1) ? A : B);
+      const int64_t lws = (t == M.nlevels - 1) ? p.q_rstride : nvecs;  // row stride of lower
       const int32_t *lm = p.i32 + L.lower_map;
       const int n_items = L.lower_rows * nvc;
       for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(kThreads) k_alm2map_legendre(LegendreParams p)
             }
           }
         }
-        double *out = lower + (int64_t)row * nvecs + v0;
+        double *out = lower + (int64_t)row * lws + v0;
 #pragma unroll
         for (int v = 0; v < VC; ++v)
           if (v < nv) out[v] = acc[v];
@@ -182,8 +184,9 @@ __global__ void __launch_bounds__(kThreads) k_map2alm_legendre(LegendreParams p)
     int idx = next_matrix(p.counter, &s_idx);
     if (idx >= p.nmats) break;
     const DevMatrix M = p.mats[p.order[idx]];
-    const double *qm = p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * nvecs;
+    const double *qm = p.q_in + (int64_t)(2 * M.m + M.odd) * p.q_mstride;
     const double *level0 = M.nlevels > 0 ? A : qm;
+    const int64_t l0s = M.nlevels > 0 ? nvecs : p.q_rstride;  // row stride of level0
     const int64_t arow0 = alm_row0(M, p.lmax);
 
     // ---- interpolation levels, leaf side to root side ----
@@ -191,6 +194,7 @@ __global__ void __launch_bounds__(kThreads) k_map2alm_legendre(LegendreParams p)
       const DevLevel L = p.levels[M.level_begin + t];
       double *upper = (t & 1) ? B : A;
       const double *lower = (t == M.nlevels - 1) ? qm : ((t & 1) ? A : B);
+      const int64_t lws = (t == M.nlevels - 1) ? p.q_rstride : nvecs;  // row stride of lower
       const int32_t *um = p.i32 + L.upper_map;
       const int n_items = L.upper_rows * nvc;
       for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
@@ -207,11 +211,11 @@ __global__ void __launch_bounds__(kThreads) k_map2alm_legendre(LegendreParams p)
           return zz < P.n_left ? (int64_t)(P.out_left + zz) : (int64_t)(P.out_right + zz - P.n_left);
         };
         double acc[VC], x[VC];
-        load_vec<VC>(acc, lower + lrow(perm[s]) * nvecs + v0, nv);
+        load_vec<VC>(acc, lower + lrow(perm[s]) * lws + v0, nv);
         const int nmk = P.n - k;
         for (int c = 0; c < nmk; ++c) {
           const double wc = w[(int64_t)c * k];
-          load_vec<VC>(x, lower + lrow(perm[k + c]) * nvecs + v0, nv);
+          load_vec<VC>(x, lower + lrow(perm[k + c]) * lws + v0, nv);
 #pragma unroll
           for (int v = 0; v < VC; ++v) acc[v] += wc * x[v];
         }
@@ -284,13 +288,13 @@ __global__ void __launch_bounds__(kThreads) k_map2alm_legendre(LegendreParams p)
           int tpo = kThreads / max(nout, 1);   // threads per output, power of two <= 32
           tpo = tpo >= 32 ? 32 : tpo >= 16 ? 16 : tpo >= 8 ? 8 : tpo >= 4 ? 4 : tpo >= 2 ? 2 : 1;
           const int per_pass = kThreads / tpo;
-          const double *X = level0 + (int64_t)(D.out_row + c0) * nvecs;
+          const double *X = level0 + (int64_t)(D.out_row + c0) * l0s;
           for (int o0 = 0; o0 < nout; o0 += per_pass) {
             const int o = o0 + threadIdx.x / tpo, lane = threadIdx.x % tpo;
             double sum = 0.0;
             const int r = o / nvecs, v = o % nvecs;
             if (o < nout)
-              for (int cc = lane; cc < gcols; cc += tpo) sum += s_tile[r][cc] * X[(int64_t)cc * nvecs + v];
+              for (int cc = lane; cc < gcols; cc += tpo) sum += s_tile[r][cc] * X[(int64_t)cc * l0s + v];
             for (int off = tpo / 2; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
             if (o < nout && lane == 0) {
               double *dst = p.alm_out + (arow0 + 2 * (int64_t)(D.row_start + k0 + r)) * nvecs + v;

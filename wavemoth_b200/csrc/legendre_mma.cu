@@ -161,14 +161,15 @@ __global__ void __launch_bounds__(kThr, 1) k_a2m_residual(FastParams p) {
         }
       }
       // epilogue: column 8 mt + g4, vectors 8 nt + 2 t4 + {0, 1}
-      double *base = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs
+      double *base = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.q_mstride
                             : p.xbuf + M.xrow * p.nvecs;
+      const int64_t rstride = G.in_q ? p.q_rstride : p.nvecs;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int cc = 8 * (warp + 8 * i) + g4;
         if (cc >= T.ncols) continue;
         const DevGCol Co = p.gcols[G.cols + T.col0 + cc];
-        double *dst = base + (int64_t)Co.row * p.nvecs + v0;
+        double *dst = base + (int64_t)Co.row * rstride + v0;
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
           const int v = 8 * nt + 2 * t4;
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(kThr) k_a2m_level(FastParams p) {
     const DevPair P = p.pairs[U.pair];
     const int K = P.kT + P.kB, K4 = (K + 3) & ~3;
     const double *X = p.xbuf + M.xrow * p.nvecs;
-    double *qm = p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs;
+    double *qm = p.q + (int64_t)(2 * M.m + M.odd) * p.q_mstride;
     const int32_t *mapT = p.i32 + P.mapT, *mapB = p.i32 + P.mapB;
     const double *ipT = p.f64 + P.ipT_t, *ipB = p.f64 + P.ipB_t;
     for (int v0 = 0; v0 < p.nvecs; v0 += VT) {
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kThr) k_a2m_level(FastParams p) {
         for (int i = 0; i < 2; ++i) {
           const int z = z0 + 16 * warp + 8 * i + g4;
           if (z >= P.n) continue;
-          double *dst = qm + (int64_t)(P.out_left + z) * p.nvecs + v0;
+          double *dst = qm + (int64_t)(P.out_left + z) * p.q_rstride + v0;
 #pragma unroll
           for (int nt = 0; nt < NT; ++nt) {
             const int v = 8 * nt + 2 * t4;
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(kThr) k_m2a_level(FastParams p) {
     const DevMatrix M = p.mats[U.matrix];
     const DevPair P = p.pairs[U.pair];
     const int n4 = (P.n + 3) & ~3;
-    const double *qm = p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs;
+    const double *qm = p.q_in + (int64_t)(2 * M.m + M.odd) * p.q_mstride;
     double *X = p.xbuf + M.xrow * p.nvecs;
     const int mtT = (P.kT + 7) / 8, mtB = (P.kB + 7) / 8, mtiles = mtT + mtB;
     for (int v0 = 0; v0 < p.nvecs; v0 += VT) {
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(kThr) k_m2a_level(FastParams p) {
       for (int idx = threadIdx.x; idx < n4 * VT; idx += kThr) {
         const int z = idx / VT, v = idx % VT;
         double val = 0.0;
-        if (z < P.n && v < vn) val = qm[(int64_t)(P.out_left + z) * p.nvecs + v0 + v];
+        if (z < P.n && v < vn) val = qm[(int64_t)(P.out_left + z) * p.q_rstride + v0 + v];
         qs[z * VP + v] = val;
       }
       __syncthreads();
@@ -329,8 +330,9 @@ __global__ void __launch_bounds__(kThr, 1) k_m2a_residual(FastParams p) {
     const DevGroup G = p.groups[T.group];
     const DevMatrix M = p.mats[G.matrix];
     const int64_t arow0 = alm_row0(M, p.lmax);
-    const double *Xb = G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs
+    const double *Xb = G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.q_mstride
                               : p.xbuf + M.xrow * p.nvecs;
+    const int64_t rstride = G.in_q ? p.q_rstride : p.nvecs;
     for (int v0 = 0; v0 < p.nvecs; v0 += VT) {
       const int vn = min(VT, p.nvecs - v0);
       double acc[PER_WARP][2];
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(kThr, 1) k_m2a_residual(FastParams p) {
             double2 val = make_double2(0.0, 0.0);
             if (c < nc && v < vn)
               val = *reinterpret_cast<const double2 *>(
-                  Xb + (int64_t)p.gcols[G.cols + c0 + c].row * p.nvecs + v0 + v);
+                  Xb + (int64_t)p.gcols[G.cols + c0 + c].row * rstride + v0 + v);
             *reinterpret_cast<double2 *>(&x_tile[c][v]) = val;
           }
         }

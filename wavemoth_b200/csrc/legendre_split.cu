@@ -291,7 +291,7 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
   DevGroup G{};
   DevPair P{};
   int K, nch;
-  int64_t plane, sidx;
+  int64_t plane, sidx, rstride;
   const double *base;
   if (kMode <= 1) {
     G = p.groups[gi];
@@ -302,7 +302,8 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
     plane = kMode == 0 ? S.apl : S.xpl;
     sidx = gi;
     if (kMode == 0) base = p.alm_in + alm_row0(M, p.lmax) * p.nvecs;
-    else base = G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs : p.xbuf + M.xrow * p.nvecs;
+    else base = G.in_q ? p.q_in + (int64_t)(2 * M.m + M.odd) * p.q_mstride : p.xbuf + M.xrow * p.nvecs;
+    rstride = (kMode == 1 && G.in_q) ? p.q_rstride : p.nvecs;
   } else {
     const DevRootUnit U = p.roots[gi];
     const DevSplitRoot R = p.sroots[gi];
@@ -312,7 +313,8 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
     nch = kMode == 2 ? R.nsc : R.nzc;
     plane = kMode == 2 ? R.b_a2m : R.b_m2a;
     sidx = (int64_t)p.ngroups + gi;
-    base = kMode == 2 ? p.xbuf + M.xrow * p.nvecs : p.q_in + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs;
+    base = kMode == 2 ? p.xbuf + M.xrow * p.nvecs : p.q_in + (int64_t)(2 * M.m + M.odd) * p.q_mstride;
+    rstride = kMode == 2 ? p.nvecs : p.q_rstride;
   }
   base += p.v0;
   auto entry = [&](int k) -> double {
@@ -322,7 +324,7 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
     else if (kMode == 1) row = p.gcols[G.cols + k].row;
     else if (kMode == 2) row = k < P.kT ? P.inT + k : P.inB + (k - P.kT);
     else row = P.out_left + k;
-    return base[row * p.nvecs + v];
+    return base[row * rstride + v];
   };
   double mx = 0.0;
   for (int k = qtr; k < K; k += 4) mx = fmax(mx, fabs(entry(k)));
@@ -669,12 +671,13 @@ __global__ void __launch_bounds__(kSplitThr, 1) k_a2m_split(SplitParams p) {
     __syncthreads();
     {
       const int vn = min(kSplitN, p.nvecs - p.v0);
-      double *base = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.ni * p.nvecs : p.xbuf + M.xrow * p.nvecs;
+      double *base = G.in_q ? p.q + (int64_t)(2 * M.m + M.odd) * p.q_mstride : p.xbuf + M.xrow * p.nvecs;
+      const int64_t rstride = G.in_q ? p.q_rstride : p.nvecs;
       for (int cc = warp; cc < T.ncols; cc += kSplitThr / 32) {
         const int row = p.gcols[G.cols + T.col0 + cc].row;
         const int vv = 2 * lane;
         if (vv < vn)
-          *reinterpret_cast<double2 *>(base + (int64_t)row * p.nvecs + p.v0 + vv) =
+          *reinterpret_cast<double2 *>(base + (int64_t)row * rstride + p.v0 + vv) =
               make_double2(xs[cc * kXsStride + vv], xs[cc * kXsStride + vv + 1]);
       }
     }

@@ -114,6 +114,9 @@ extern "C" int wavemoth_legendre_alm2map_noalloc(wavemoth_plan plan, const doubl
   p.scratch = (double *)((unsigned char *)base + kCounterBytes);
   p.alm_in = alm;
   p.q_out = q;
+  // the caller's q is in the layout of wavemoth_get_work: row (2m + parity) ni + ring
+  p.q_mstride = (int64_t)p.ni * p.nvecs;
+  p.q_rstride = p.nvecs;
   cudaError_t e = cudaMemsetAsync(base, 0, sizeof(int32_t), st);
   if (e == cudaSuccess) e = wm::launch_legendre(true, p, nslots, st);
   if (e != cudaSuccess)

@@ -453,7 +453,6 @@ namespace wm {
 // 0) or of the X buffer (depth 1), map2alm residual rows of the alm, level
 // rows of q (alm2map) or of the X buffer (map2alm).
 static void build_stream_tables(HostProgram &P) {
-  const int64_t ni = 2 * (int64_t)P.nside;
   for (int k = 0; k < 4; ++k) {
     P.stream_tiles[k].clear();
     P.stream_rows[k].clear();
@@ -470,10 +469,10 @@ static void build_stream_tables(HostProgram &P) {
     const DevGroup &G = P.groups[T.group];
     const DevSplitGroup &S = P.sgroups[T.group];
     const DevMatrix &M = P.mats[G.matrix];
-    const int64_t base = G.in_q ? (int64_t)(2 * M.m + M.odd) * ni : (int64_t)M.xrow;
     for (int r = 0; r < kSplitM; ++r) {
       const bool act = r < T.ncols;
-      rows[r] = act ? (int32_t)(base + P.gcols[G.cols + T.col0 + r].row) : -1;
+      const int32_t gr = act ? P.gcols[G.cols + T.col0 + r].row : 0;
+      rows[r] = act ? (int32_t)(G.in_q ? q_row(P, M.m, M.odd, gr) : M.xrow + gr) : -1;
       sidx[r] = act ? (int32_t)(G.cols + T.col0 + r) : -1;
     }
     const int32_t nk = S.nrchunks - T.kc0;
@@ -507,7 +506,7 @@ static void build_stream_tables(HostProgram &P) {
         const bool act = r < T.nrows;
         const int32_t rr = T.row0 + r;
         int64_t dst = -1;
-        if (act && a2m) dst = (int64_t)(2 * M.m + M.odd) * ni + pr.out_left + rr;
+        if (act && a2m) dst = q_row(P, M.m, M.odd, pr.out_left + rr);
         if (act && !a2m) dst = (int64_t)M.xrow + (rr < pr.kT ? pr.inT + rr : pr.inB + (rr - pr.kT));
         rows[r] = (int32_t)dst;
         sidx[r] = act ? (int32_t)((a2m ? R.rs_a2m : R.rs_m2a) + rr) : -1;
@@ -529,7 +528,6 @@ static void build_split_tables(HostProgram &P) {
   std::vector<std::pair<int32_t, DevSplitTileA>> ta;
   std::vector<std::pair<int32_t, DevSplitTileB>> tb;
   for (auto &z : P.split_zero) z.clear();
-  const int64_t ni = 2 * (int64_t)P.nside;
   auto zero = [&](int launch, int64_t buf, int64_t row) {
     P.split_zero[launch].push_back((buf << kZeroBufShift) | row);
   };
@@ -555,9 +553,10 @@ static void build_split_tables(HostProgram &P) {
       } else {
         // no active row in any column of the tile: its outputs are zero
         const DevMatrix &M = P.mats[G.matrix];
-        const int64_t base = G.in_q ? (int64_t)(2 * M.m + M.odd) * ni : (int64_t)M.xrow;
-        for (int32_t c = c0; c < c0 + T.ncols; ++c)
-          zero(kStreamResA2M, G.in_q ? 0 : 1, base + P.gcols[G.cols + c].row);
+        for (int32_t c = c0; c < c0 + T.ncols; ++c) {
+          const int32_t gr = P.gcols[G.cols + c].row;
+          zero(kStreamResA2M, G.in_q ? 0 : 1, G.in_q ? q_row(P, M.m, M.odd, gr) : M.xrow + gr);
+        }
       }
     }
     if (S.ncchunks > 0) {
@@ -608,7 +607,7 @@ static void build_split_tables(HostProgram &P) {
     } else {
       // a root without skeleton rows: its q rows are zero
       const DevMatrix &M = P.mats[P.roots[u].matrix];
-      for (int32_t z = 0; z < pr.n; ++z) zero(kStreamLevelA2M, 0, (int64_t)(2 * M.m + M.odd) * ni + pr.out_left + z);
+      for (int32_t z = 0; z < pr.n; ++z) zero(kStreamLevelA2M, 0, q_row(P, M.m, M.odd, pr.out_left + z));
     }
     if (R.nzc > 0)
       for (int32_t s0 = 0; s0 < K; s0 += kSplitM)

@@ -58,6 +58,14 @@ struct HostProgram {
   int64_t aux_values = 0;        // recurrence coefficients stored
 };
 
+// Row of q (rows of nvecs doubles) holding (m, parity, ring): ring-major, so
+// that the q block of one ring pair -- every (m, parity) of it -- is one
+// contiguous range (rows ring * 2 (mmax + 1) .. + 2 (mmax + 1)).
+inline int64_t q_row(int mmax, int m, int odd, int64_t ring) {
+  return (ring * (mmax + 1) + m) * 2 + odd;
+}
+inline int64_t q_row(const HostProgram &P, int m, int odd, int64_t ring) { return q_row(P.mmax, m, odd, ring); }
+
 // Streamed split GEMM launches.
 enum : int { kStreamResA2M = 0, kStreamResM2A = 1, kStreamLevelA2M = 2, kStreamLevelM2A = 3 };
 

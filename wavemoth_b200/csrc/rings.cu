@@ -447,8 +447,9 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
   cplx *phi = plo + kPhaseLo;
   phase_tables(plo, phi, p, c.ring);
   __syncthreads();
-  const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
-  const double *qbase = p.q + (int64_t)c.ring * p.nvecs + 2 * c.map0;
+  // q rows are ring-major: (m, parity) of ring r at row (r (mmax + 1) + m) 2 + parity
+  const int64_t half = p.nvecs, qstride = 2 * half;
+  const double *qbase = p.q + (int64_t)c.ring * (p.mmax + 1) * qstride + 2 * c.map0;
   const Radices rs = radices(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
@@ -562,8 +563,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   cplx *plo = buf + ((int64_t)M << lg);
   cplx *phi = plo + kPhaseLo;
   phase_tables(plo, phi, p, c.ring);
-  const int64_t half = (int64_t)p.ni * p.nvecs, qstride = 2 * half;
-  double *qbase = p.q_out + (int64_t)c.ring * p.nvecs + 2 * c.map0;
+  const int64_t half = p.nvecs, qstride = 2 * half;
+  double *qbase = p.q_out + (int64_t)c.ring * (p.mmax + 1) * qstride + 2 * c.map0;
   const Radices rs = radices(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
