@@ -16,6 +16,7 @@
 #ifndef WAVEMOTH_B200_WAVEMOTH_H
 #define WAVEMOTH_B200_WAVEMOTH_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -83,6 +84,84 @@ void wavemoth_perform_backward_ffts(wavemoth_plan plan);
 
 /* Sets every phi0 to zero (test hook).  Replaces src/wavemoth_private.h:138. */
 void wavemoth_disable_phase_shifting(wavemoth_plan plan);
+
+/* ---- kernel-level hooks (src/legendre_transform.h, src/butterfly.h.in) ----
+   Host pointers throughout.  The two that compute (the Legendre transform and
+   the butterfly transposed apply) run on the current CUDA device: inputs are
+   copied up, one of this library's kernels runs, the output is copied back.
+   Errors are reported through wavemoth_last_error() (and, for
+   bfm_transpose_apply_d, its return code) instead of abort(). */
+
+/* (alpha, beta, gamma) of the even/odd three-term recurrence for rows
+   l = lmin + 2k, k = 2 .. nk-1: 3 (nk - 2) values.  Replaces
+   src/legendre_transform.h:16-17 (legendre_transform.c.in:723-747). */
+void wavemoth_legendre_transform_auxdata(size_t m, size_t lmin, size_t nk, double *auxdata);
+
+/* y[i, j] = sum_{k < nk} P_k(x_i) a[2k, j] with P_0 = P[i], P_1 = Pp1[i] and
+   P_k from the recurrence; a has row stride 2 nvecs (every other row is
+   used), y is (nx, nvecs).  Same operations in the same order as the
+   reference's scalar routine, so the same y bit for bit.  Replaces
+   src/legendre_transform.h:19-26 (legendre_transform.c.in:680-716). */
+void wavemoth_legendre_transform(size_t nx, size_t nl, size_t nvecs, double *a_l, double *y,
+                                 double *x_squared, double *auxdata, double *P, double *Pp1);
+
+/* The same transform with a_l in the layout of
+   wavemoth_legendre_transform_pack; nvecs even; work is not used.  Replaces
+   src/legendre_transform.h:28-35 (legendre_transform.c.in:640-678). */
+void wavemoth_legendre_transform_sse(size_t nx, size_t nl, size_t nvecs, double *a_l, double *y,
+                                     double *x_squared, double *auxdata, double *P, double *Pp1,
+                                     char *work);
+
+/* The reference's work-buffer size for the transform above (0 for
+   nvecs == 2).  Replaces src/legendre_transform.h:37
+   (legendre_transform.c.in:625-633). */
+size_t wavemoth_legendre_transform_sse_query_work(size_t nvecs);
+
+/* Packs rows 0, 2, 4, ... of input (row stride 2 nvecs) into the reference's
+   blocked layout: rows 0-1, then chunks of 42 rows; within a chunk blocks of
+   4 vectors, row after row.  Replaces src/legendre_transform.h:39-40
+   (legendre_transform.c.in:330-380). */
+void wavemoth_legendre_transform_pack(size_t nk, size_t nvecs, double *input, double *output);
+
+/* Residual-block callback of the transposed apply: fill rows [start, stop)
+   of buf (nvecs doubles each) from the payload.  Same type as
+   src/butterfly.h.in:116-117. */
+typedef void (*pull_func_t)(double *buf, size_t start, size_t stop, size_t nvecs, char *payload,
+                            size_t payload_len, void *ctx);
+
+typedef struct _bfm_plan bfm_plan;
+
+/* Header fields of a serialized butterfly matrix; same fields as
+   src/butterfly.h.in:152-155. */
+typedef struct {
+  size_t nrows, ncols, k_max, nblocks_max, element_count;
+  size_t first_level_size, heap_size, heap_first_index;
+} bfm_matrix_data_info;
+
+/* Plan of the transposed apply (sizes only; the semaphores of the
+   reference's NUMA scheduling are not used and may be NULL).  Replaces
+   src/butterfly.h.in:141-143 and :144. */
+bfm_plan *bfm_create_plan(size_t k_max, size_t nblocks_max, size_t nvecs, void *mem_semaphore,
+                          void *cpu_semaphore);
+void bfm_destroy_plan(bfm_plan *plan);
+
+/* target (ncols, nvecs) = A^T x for the serialized butterfly matrix A at
+   matrix_data (16-byte aligned), the residual blocks supplied by pull_func
+   in the reference's order; 0 on success.  Replaces src/butterfly.h.in:146-151
+   (butterfly.c.in:375-432). */
+int bfm_transpose_apply_d(bfm_plan *plan, char *matrix_data, pull_func_t pull_func, double *target,
+                          size_t target_len, void *caller_ctx);
+
+/* Reads the 40-byte matrix header; returns the pointer just after it.
+   Replaces src/butterfly.h.in:157 (butterfly.c.in:434-445). */
+char *bfm_query_matrix_data(char *head, bfm_matrix_data_info *info);
+
+/* Copies (or adds, should_add) the consecutive rows of source to the rows of
+   target1 (mask entries 0 .. len1-1) and target2 (the next len2 entries)
+   whose mask entry equals group; returns the mask after the last entry read.
+   Replaces src/butterfly.h.in:178-184 (butterfly.c.in:57-139). */
+const char *bfm_scatter(const char *mask, double *target1, double *target2, const double *source,
+                        size_t len1, size_t len2, size_t nvecs, int group, int should_add);
 
 #ifdef __cplusplus
 }

@@ -141,6 +141,31 @@ int64_t wavemoth_plan_image_bytes(wavemoth_plan plan);
    exercise allocation-failure handling without exhausting the GPU. */
 void wavemoth_set_device_memory_cap(int64_t bytes);
 
+/* Quadrature weights of the analysis direction: weights[r] (r = 0 .. 2 Nside
+   - 1, ring pairs from the equator; positive) multiplies the pixels of the
+   rings mid - r and mid + r in map2alm, a_lm = 4 pi / Npix sum_p w_r(p) f_p
+   lambda_lm(theta_p) e^{-i m phi_p}.  NULL restores unit weights.  Host
+   pointer; copied.  The alm2map direction is unchanged.  New: the reference
+   has no analysis direction. */
+int wavemoth_plan_set_ring_weights(wavemoth_plan plan, const double *weights);
+
+/* map2alm refined by niter Jacobi iterations, a_{k+1} = a_k +
+   map2alm(f - alm2map(a_k)), on device buffers (layouts as
+   wavemoth_execute_map2alm_device) on `stream`.  The first call with
+   niter > 0 allocates two plan-owned buffers (a map and an alm).  With ring
+   weights set, every map2alm of the iteration is weighted.  New. */
+int wavemoth_map2alm_iterative_device(wavemoth_plan plan, const double *map, double *alm, int niter,
+                                      void *stream);
+
+/* The adjoint of the plan's transform on its bound buffers: reads the
+   output buffer, writes the input buffer.  alm2map plan: alm = (Npix / 4 pi)
+   map2alm(map); map2alm plan: map = (4 pi / Npix) alm2map(alm) -- the
+   adjoints with respect to the real inner product on maps and
+   <a, b> = sum_lm c_m Re(a_lm conj b_lm), c_0 = 1, c_m = 2, on alm.  Status
+   through wavemoth_plan_status.  New: the reference has no analysis
+   direction (src/wavemoth.c:1271-1283 is synthesis only). */
+void wavemoth_execute_adjoint(wavemoth_plan plan);
+
 /* Test hook: how many times a wait of the streamed split-precision GEMM
    (wavemoth_execute_*_device with WAVEMOTH_PRECISION_SPLIT) polls its
    mbarrier for another warp role before it gives up (0 restores the

@@ -25,7 +25,7 @@ def declared_functions():
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"\b([a-z_][a-z0-9_]*)\s*\(", text):
             name = m.group(1)
-            if name.startswith(("wavemoth_", "wm_")):
+            if name.startswith(("wavemoth_", "wm_", "bfm_")):
                 names.add(name)
     return sorted(names)
 

@@ -98,3 +98,26 @@ def test_c_grid_table_matches():
     ref = pytest.importorskip("oracle.ref")
     if ref.available():
         np.testing.assert_array_equal(ref.phi0s(16), phi0)
+
+
+def test_ring_weights_integrate_zonal_harmonics():
+    """Ring weights (wavemoth_b200.weights): the weighted ring sum integrates
+    Y_l0, l even <= 2 nside, exactly (checked against an independent
+    Legendre evaluation: numpy's Legendre series, lambda_l0 = sqrt((2l+1)/4pi)
+    P_l(cos theta)), and stays close to unit weights."""
+    import numpy as np
+    from numpy.polynomial import legendre as L
+    from wavemoth_b200 import weights
+    from wavemoth_b200.healpix import get_ring_pixel_counts, get_ring_thetas
+    for nside in (4, 16, 32):
+        w = weights.ring_weights(nside)
+        th = get_ring_thetas(nside, positive_only=True)
+        n = get_ring_pixel_counts(nside)[2 * nside - 1:]
+        c = np.where(np.arange(2 * nside) == 0, 1.0, 2.0)
+        for l in range(0, 2 * nside + 1, 2):
+            coef = np.zeros(l + 1)
+            coef[l] = 1.0
+            ylm = np.sqrt((2 * l + 1) / (4 * np.pi)) * L.legval(np.cos(th), coef)
+            q = 4 * np.pi / (12 * nside * nside) * np.sum(c * n * w * ylm)
+            assert abs(q - (np.sqrt(4 * np.pi) if l == 0 else 0.0)) < 1e-12
+        assert 0.9 < w.min() and w.max() < 1.15

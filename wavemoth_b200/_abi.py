@@ -4,6 +4,9 @@ import ctypes
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+# pull_func_t of bfm_transpose_apply_d (src/butterfly.h.in:116-117)
+PULL_FUNC = ctypes.CFUNCTYPE(None, _dp, _sz, _sz, _sz, _vp, _sz, _vp)
 
 SIGNATURES = {
     "wavemoth_configure": (None, [ctypes.c_char_p]),
@@ -38,6 +41,20 @@ SIGNATURES = {
     "wavemoth_plan_image_bytes": (ctypes.c_int64, [_vp]),
     "wavemoth_set_device_memory_cap": (None, [ctypes.c_int64]),
     "wavemoth_plan_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_int64]),
+    "wavemoth_execute_adjoint": (None, [_vp]),
+    "wavemoth_plan_set_ring_weights": (ctypes.c_int, [_vp, _dp]),
+    "wavemoth_map2alm_iterative_device": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    # kernel-level hooks (src/legendre_transform.h, src/butterfly.h.in)
+    "wavemoth_legendre_transform_auxdata": (None, [_sz, _sz, _sz, _dp]),
+    "wavemoth_legendre_transform": (None, [_sz, _sz, _sz, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "wavemoth_legendre_transform_sse": (None, [_sz, _sz, _sz, _dp, _dp, _dp, _dp, _dp, _dp, _vp]),
+    "wavemoth_legendre_transform_sse_query_work": (_sz, [_sz]),
+    "wavemoth_legendre_transform_pack": (None, [_sz, _sz, _dp, _dp]),
+    "bfm_create_plan": (_vp, [_sz, _sz, _sz, _vp, _vp]),
+    "bfm_destroy_plan": (None, [_vp]),
+    "bfm_transpose_apply_d": (ctypes.c_int, [_vp, _vp, PULL_FUNC, _dp, _sz, _vp]),
+    "bfm_query_matrix_data": (_vp, [_vp, _vp]),
+    "bfm_scatter": (_vp, [_vp, _dp, _dp, _dp, _sz, _sz, _sz, ctypes.c_int, ctypes.c_int]),
     "wavemoth_legendre_alm2map_noalloc": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_plan_timing": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "wavemoth_plan_kernel_launches": (ctypes.c_int64, [_vp]),

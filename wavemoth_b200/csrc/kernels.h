@@ -31,6 +31,8 @@ struct LegendreParams {
   double *scratch;        // gridDim.x slots of slot_stride doubles
   int64_t slot_stride;    // 2 * max_rows * nvecs
   int32_t *counter;       // work queue head (zeroed before launch)
+  int32_t level0_given;   // alm2map: the root rows are already in each CTA's first buffer
+                          // (the residual stage is skipped; trees of depth >= 1 only)
 };
 
 struct FastParams {
@@ -154,6 +156,8 @@ struct RingParams {
   const double *map_in;   // analysis input (npix, nmaps)
   double *q_out;          // analysis output
   double scale;           // analysis: multiplies q~ (4 pi / npix for map2alm)
+  double map_scale;       // synthesis: multiplies the map (1 for alm2map)
+  const double *ring_weights;  // analysis: per ring pair, multiplies q~ (quadrature weights; null: 1)
   int32_t phase_shifts;   // 0 disables e^{i m phi0} (test hook)
   const double2 *twiddles;  // e^{2 pi i k / twlen}, k < twlen / 2
   int32_t twlen;
@@ -175,6 +179,10 @@ struct RingParams {
 };
 
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
+// y = a - b (n doubles), and y += x (n doubles): the steps of the iterative
+// map2alm between the transforms
+cudaError_t launch_residual(const double *a, const double *b, double *y, int64_t n, cudaStream_t st);
+cudaError_t launch_accumulate(const double *x, double *y, int64_t n, cudaStream_t st);
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
                               double *aux, double2 *phases, cudaStream_t st);

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kThreads) k_alm2map_legendre(LegendreParams p)
 
     // ---- residual stage: one item per (depth-0 row, vector chunk) ----
     const int32_t *rmap = p.i32 + M.root_map;
-    const int nitems = M.root_rows * nvc;
+    const int nitems = p.level0_given ? 0 : M.root_rows * nvc;
     for (int it = threadIdx.x; it < nitems; it += blockDim.x) {
       const int row = it % M.root_rows, v0 = (it / M.root_rows) * VC;
       const int nv = min(VC, nvecs - v0);

@@ -66,7 +66,7 @@ size_t append_i32(std::vector<int32_t> &arena, const std::vector<int32_t> &v) {
 }
 
 bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int ncols_expect,
-                    HostProgram &P) {
+                    HostProgram &P, bool tree_only = false) {
   if (start % 16 != 0) return R.fail("matrix data not 16-byte aligned");
   int32_t nrows = R.get<int32_t>(start + 0, "matrix header");
   int32_t ncols = R.get<int32_t>(start + 4, "matrix header");
@@ -265,7 +265,8 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
   }
 
   // ---- residual blocks of every forest root ----
-  for (int r = 0; r < nroots; ++r) {
+  // (tree_only: the caller supplies the root rows; no payload is decoded)
+  for (int r = 0; r < nroots && !tree_only; ++r) {
     const NodeInfo &root = nodes[0][r];
     int nb = (int)root.heights.size();
     if (res_off[r] <= 0) return R.fail("missing residual payload table");
@@ -355,7 +356,7 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
     }
   }
   M.dblock_end = (int32_t)P.dblocks.size();
-  {
+  if (!tree_only) {
     std::vector<int32_t> rm(2 * (size_t)M.root_rows, -1);
     for (int32_t b = M.dblock_begin; b < M.dblock_end; ++b) {
       const DevDBlock &D = P.dblocks[b];
@@ -381,6 +382,17 @@ bool compile_matrix(Reader &R, size_t start, int m, int odd, int nk_expect, int 
 }
 
 }  // namespace
+
+bool compile_butterfly_tree(const char *data, size_t len, HostProgram &P, std::string &err) {
+  Reader R{data, len, &err};
+  const int32_t nrows = R.get<int32_t>(0, "matrix header"), ncols = R.get<int32_t>(4, "matrix header");
+  if (!R.ok) return false;
+  P = HostProgram{};
+  P.element_count.assign(2, 0);
+  if (!compile_matrix(R, 0, 0, 0, nrows, ncols, P, true)) return false;
+  P.max_rows = P.mats[0].max_rows;
+  return true;
+}
 
 bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_expect,
                       int mmax_expect, HostProgram &P, std::string &err) {

@@ -72,6 +72,11 @@ enum : int { kStreamResA2M = 0, kStreamResM2A = 1, kStreamLevelA2M = 2, kStreamL
 // Builds the tensor-core path tables for matrices of depth 0 and 1.
 bool build_fast_path(HostProgram &P, std::string &err);
 
+// One serialized butterfly matrix (the per-matrix layout of a rev1 file,
+// starting at its header) compiled without its residual payloads: a single
+// DevMatrix whose root buffer rows the caller provides.
+bool compile_butterfly_tree(const char *data, size_t len, HostProgram &P, std::string &err);
+
 // Parses a rev1 file image.  nside_expect < 0 accepts any nside.
 bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_expect,
                       int mmax_expect, HostProgram &P, std::string &err);

@@ -52,6 +52,8 @@
 // group of 16 that makes the 16-byte accesses of every pass of radix 2..16
 // conflict-free for 1, 2, 4, 8 and 16 lanes.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "plan.h"
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
   const Radices rs = radices(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
-  const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
+  const double inv = (c.pow2 ? 1.0 : 1.0 / (double)M) * p.map_scale;
   const int gmm = (1 << c.lgm) - 1;
   for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;  // the equator is written once
@@ -523,6 +525,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
     // pixels 2s, 2s + 1 of output z[s]; power of two: DIF position pos holds z[bitrev(pos)]
     auto pix_dif = [&](int pos, int g, cplx z) {
       if (!lane_live(c, g, side)) return;
+      z = cscale(z, p.map_scale);
       const int64_t s2 = 2 * (int64_t)bitrev((unsigned)pos, c.bits);
       *out_row(g, s2) = z.x;
       *out_row(g, s2 + 1) = z.y;
@@ -571,6 +574,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
   const int gmm = (1 << c.lgm) - 1;
   const bool npow2 = (n & (n - 1)) == 0;  // every belt ring when nside is a power of two
+  // 4 pi / npix, times the ring's quadrature weight when weights are set
+  const double wscale = p.ring_weights ? p.scale * p.ring_weights[c.ring] : p.scale;
   for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;
     auto in_row = [&](int g, int64_t pix) -> const double * {
@@ -629,7 +634,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
       const cplx O = {0.5 * D.y, -0.5 * D.x};  // D / (2i)
       cplx Fk = cadd(E, cmul(cconj(ring_root(p, c.R, k)), O));
       if (mirror) Fk = cconj(Fk);
-      return cscale(cmul(Fk, cconj(phase_at(plo, phi, m))), p.scale);
+      return cscale(cmul(Fk, cconj(phase_at(plo, phi, m))), wscale);
     };
     for (int t = threadIdx.x; t < ((p.mmax + 1) << c.lgm); t += blockDim.x) {
       const int mi = t & gmm, m = t >> c.lgm;
@@ -737,6 +742,29 @@ cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st) {
 
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st) {
   return launch_rings(k_ring_analysis, prm, st);
+}
+
+__global__ void k_residual(const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ y,
+                           int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = a[i] - b[i];
+}
+
+__global__ void k_accumulate(const double *__restrict__ x, double *__restrict__ y, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+cudaError_t launch_residual(const double *a, const double *b, double *y, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_residual<<<(unsigned)std::min<int64_t>((n + 255) / 256, 8192), 256, 0, st>>>(a, b, y, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate(const double *x, double *y, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_accumulate<<<(unsigned)std::min<int64_t>((n + 255) / 256, 8192), 256, 0, st>>>(x, y, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters, double *aux,

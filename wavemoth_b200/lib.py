@@ -112,6 +112,13 @@ class ShtPlan:
             self._check("execute")
         return self.output
 
+    def execute_adjoint(self):
+        """The adjoint of execute on the bound buffers: reads the output
+        buffer, writes the input buffer (wavemoth_execute_adjoint)."""
+        _lib().wavemoth_execute_adjoint(self._plan)
+        self._check("execute_adjoint")
+        return self.input
+
     def perform_legendre_transform(self, repeat=1):
         for _ in range(repeat):
             _lib().wavemoth_perform_legendre_transforms(self._plan)

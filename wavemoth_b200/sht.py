@@ -64,15 +64,39 @@ class Transform:
             raise WavemothError("alm2map failed (%d): %s" % (rc, last_error()))
         return out
 
-    def map2alm(self, maps, out=None):
+    def map2alm(self, maps, out=None, niter=0):
+        """a = 4 pi / Npix A^T f (times the ring weights, if set); niter > 0
+        refines it by Jacobi iterations a += map2alm(f - alm2map(a))."""
         maps = self._check_map(maps)
         if out is None:
             out = torch.empty((self.nalm, self.nmaps), dtype=torch.complex128, device=maps.device)
-        rc = _native.lib().wavemoth_execute_map2alm_device(
-            self._plans["map2alm"], maps.data_ptr(), out.data_ptr(), self._stream())
+        if niter:
+            rc = _native.lib().wavemoth_map2alm_iterative_device(
+                self._plans["map2alm"], maps.data_ptr(), out.data_ptr(), int(niter), self._stream())
+        else:
+            rc = _native.lib().wavemoth_execute_map2alm_device(
+                self._plans["map2alm"], maps.data_ptr(), out.data_ptr(), self._stream())
         if rc != 0:
             raise WavemothError("map2alm failed (%d): %s" % (rc, last_error()))
         return out
+
+    def set_ring_weights(self, weights):
+        """Quadrature weights of the 2 Nside ring pairs (equator first) used by
+        map2alm (wavemoth_b200.weights.ring_weights), or None for unit
+        weights."""
+        import ctypes
+
+        import numpy as np
+        if weights is None:
+            rc = _native.lib().wavemoth_plan_set_ring_weights(self._plan, None)
+        else:
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+            if w.shape != (2 * self.nside,):
+                raise ValueError("weights must have shape (%d,)" % (2 * self.nside))
+            rc = _native.lib().wavemoth_plan_set_ring_weights(
+                self._plan, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if rc != 0:
+            raise WavemothError("set_ring_weights failed: " + last_error())
 
     def device_status(self):
         """Waits for torch's current stream and raises if a kernel recorded an
