@@ -57,6 +57,10 @@ def parse():
                     help="uneven batch instead of the headline workload: --requests seeded requests "
                          "(nside from --uneven-nsides, lmax = 2 nside, 1-8 maps, split alm2map) as one "
                          "graph launch, against the same requests called one after another")
+    ap.add_argument("--compare-dense", action="store_true",
+                    help="round-trip maps/s of dense-recurrence plans (no butterfly file) against "
+                         "butterfly plans at each of --dense-nsides (lmax = 2 nside), both precisions")
+    ap.add_argument("--dense-nsides", default="32,64,128,256,512")
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--uneven-nsides", default="64,128,256,512")
     ap.add_argument("--no-parity", action="store_true",
@@ -678,10 +682,53 @@ def run_uneven(a):
     print(json.dumps(line), flush=True)
 
 
+def run_compare_dense(a):
+    """Dense-recurrence plans against butterfly plans: one round trip of
+    a.nmaps maps per step, device-resident inputs, CUDA-event timed."""
+    import types
+
+    import torch
+    from wavemoth_b200.sht import Transform
+    rows = []
+    for nside in [int(x) for x in a.dense_nsides.split(",")]:
+        lmax = 2 * nside
+        pa = types.SimpleNamespace(nside=nside, lmax=lmax, eps=a.eps, chunk=a.chunk, memop=a.memop,
+                                   plan_dir=a.plan_dir)
+        path = ensure_plan(pa, 0)
+        alm = torch.from_numpy(synthetic_alm(lmax, a.nmaps, 1000)).cuda()
+        row = {"nside": nside, "lmax": lmax}
+        for prec in ("double", "split"):
+            for kind in ("butterfly", "dense"):
+                T = Transform(None if kind == "dense" else path, nside, lmax, a.nmaps, precision=prec,
+                              dense=kind == "dense")
+                maps = torch.empty((T.npix, a.nmaps), dtype=torch.float64, device="cuda")
+                out = torch.empty_like(alm)
+                for _ in range(a.warmup):
+                    T.alm2map(alm, out=maps)
+                    T.map2alm(maps, out=out)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(a.steps):
+                    T.alm2map(alm, out=maps)
+                    T.map2alm(maps, out=out)
+                e1.record()
+                torch.cuda.synchronize()
+                T.device_status()
+                row["%s_%s_maps_per_s" % (kind, prec)] = a.nmaps * a.steps / (e0.elapsed_time(e1) / 1e3)
+                T.close()
+        rows.append(row)
+        log(json.dumps(row))
+    print(json.dumps({"metric": "alm2map+map2alm maps/sec, dense-recurrence vs butterfly plans",
+                      "unit": "maps/s", "nmaps": a.nmaps, "steps": a.steps, "rows": rows}), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.compare_dense:
+        run_compare_dense(a)
     elif a.uneven:
         run_uneven(a)
     else:

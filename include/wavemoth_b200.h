@@ -22,6 +22,10 @@ extern "C" {
 #define WAVEMOTH_PRECISION_SPLIT 0x200   /* residual products of depth-0/1 matrices as sliced int8
                                             tensor-core GEMMs re-summed in FP64 (Ozaki scheme);
                                             the recurrence, seeds and scales stay FP64 */
+#define WAVEMOTH_DENSE 0x800            /* no butterfly file: every (m, parity) block as one dense
+                                           three-term recurrence over all rings, seeded on the device
+                                           (the reference GPU kernel's scheme, wavemoth/cuda/sht.py:20-148);
+                                           resource_filename is ignored, Nside must be given */
 #define WAVEMOTH_SPLIT_GENERATE 0x400    /* with WAVEMOTH_PRECISION_SPLIT: generate the residual P
                                             inside the GEMM kernels at every call instead of
                                             slicing it once per plan into device memory (6 bytes

@@ -137,6 +137,14 @@ cudaError_t launch_zero_rows(const SplitParams &prm, const int64_t *rows, int32_
 cudaError_t launch_split_scales(const SplitParams &prm, cudaStream_t st);
 cudaError_t launch_level_slices(const SplitParams &prm, cudaStream_t st);
 
+// Dense-recurrence plans (dense.cu): first stored row of every (m, parity,
+// ring) column, kstart[(2m + parity) ni + ring], for lambda_lm > eps; then
+// the stored values written into the plan's FP64 arena.
+cudaError_t launch_dense_scan(int lmax, int mmax, const double *thetas, int ni, double eps, int32_t *kstart,
+                              cudaStream_t st);
+cudaError_t launch_dense_fill(int lmax, int mmax, const double *thetas, int ni, double eps, const int32_t *kstart,
+                              const DevDenseFill *fill, double *f64, cudaStream_t st);
+
 int legendre_threads();
 cudaError_t legendre_preload();
 // Device address and size of the allocation-free entry point's static

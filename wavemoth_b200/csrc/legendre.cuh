@@ -38,14 +38,16 @@ WM_HD double rec_r0(int l, int m) {
   return sqrt(4.0 * (l + 1) * (l + 1) - 1.0) / sqrt((double)(l + m + 1) * (double)(l - m + 1));
 }
 
-// Fills out[l - m] for l = m..lmax.  theta in [0, pi].
-// Returns the first l with a value stored (lmax + 1 if all zero).
-WM_HD int legendre_column(int m, double theta, int lmax, double eps, double *out) {
+// Walks lambda_lm(theta) for l = m..lmax and calls visit(l, value) for every
+// l from the first with |value| > eps on (the values before it are zero);
+// stops early when visit returns false.  theta in [0, pi].  Returns that
+// first l (lmax + 1 if all values are zero).
+template <class Visit>
+WM_HD int legendre_walk(int m, double theta, int lmax, double eps, Visit &&visit) {
   const double pi = 3.14159265358979323846;
   if (theta == 0.0) theta = 1e-16;
   if (fabs(theta - pi) < 1e-15) theta = pi - 1e-15;
   double cth = cos(theta), sth = sin(theta);
-  for (int l = m; l <= lmax; ++l) out[l - m] = 0.0;
   if (m > 0 && sth == 0.0) return lmax + 1;
 
   double lg = log2_pmm_prefactor(m);
@@ -89,13 +91,23 @@ WM_HD int legendre_column(int m, double theta, int lmax, double eps, double *out
     ++l;
   }
   int first = l;
-  out[l - m] = cur;
+  if (!visit(l, cur)) return first;
   while (l + 1 <= lmax) {
     step(l);
     ++l;
-    out[l - m] = cur;
+    if (!visit(l, cur)) break;
   }
   return first;
+}
+
+// Fills out[l - m] for l = m..lmax (zero before the first |value| > eps).
+// Returns the first l with a value stored (lmax + 1 if all zero).
+WM_HD int legendre_column(int m, double theta, int lmax, double eps, double *out) {
+  for (int l = m; l <= lmax; ++l) out[l - m] = 0.0;
+  return legendre_walk(m, theta, lmax, eps, [&](int l, double v) {
+    out[l - m] = v;
+    return true;
+  });
 }
 
 // Recurrence coefficients of the even/odd (step-2) three-term recurrence

@@ -161,6 +161,16 @@ struct DevSplitRoot {
   int32_t nzc, nsc;         // chunks of 64 over z and over s
 };
 
+// Dense-recurrence plans: where the device Legendre seeds of column (m,
+// parity, ring) go in the FP64 arena -- the value at row kstart + t, t <
+// count, at base + t stride (P0 and P1 of a recurrence strip: count 2,
+// stride nx; a dense strip of nks rows: count nks, stride 1).
+struct DevDenseFill {
+  int64_t base;
+  int32_t stride;
+  int32_t count;
+};
+
 // Rows that no split tile writes, zeroed before the launch they belong to:
 // (buffer << kZeroBufShift) | row, buffer 0 q, 1 X buffer, 2 alm.
 constexpr int kZeroBufShift = 56;

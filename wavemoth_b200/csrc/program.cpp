@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "legendre.cuh"
 #include "plan.h"
 #include "program.h"
 
@@ -391,6 +392,125 @@ bool compile_butterfly_tree(const char *data, size_t len, HostProgram &P, std::s
   P.element_count.assign(2, 0);
   if (!compile_matrix(R, 0, 0, 0, nrows, ncols, P, true)) return false;
   P.max_rows = P.mats[0].max_rows;
+  return true;
+}
+
+std::vector<double> ring_pair_z(int nside) {
+  std::vector<double> z(2 * (size_t)nside);
+  const double ns = (double)nside;
+  for (int r = 0; r < 2 * nside; ++r) {
+    const double i = (double)(2 * nside - r);  // ring number counted from the north pole, from 1
+    z[r] = i <= ns ? 1.0 - i * i / (3.0 * ns * ns) : 4.0 / 3.0 - 2.0 * i / (3.0 * ns);
+  }
+  return z;
+}
+
+bool build_dense_program(int nside, int lmax, int mmax, const std::vector<int32_t> &kstart, HostProgram &P,
+                         std::vector<DevDenseFill> &fill, std::string &err) {
+  const int ni = 2 * nside;
+  if (nside <= 0 || lmax < 0 || mmax > lmax || kstart.size() != 2 * (size_t)(mmax + 1) * ni) {
+    err = "dense program: inconsistent sizes";
+    return false;
+  }
+  P = HostProgram{};
+  P.nside = nside;
+  P.lmax = lmax;
+  P.mmax = mmax;
+  P.element_count.assign(2 * (mmax + 1), 0);
+  fill.assign(kstart.size(), DevDenseFill{0, 0, 0});
+  const std::vector<double> z = ring_pair_z(nside);
+  auto zeros = [&](size_t n) {
+    const size_t off = (P.f64.size() + 3) & ~size_t(3);
+    P.f64.resize(off + n, 0.0);
+    return (int64_t)off;
+  };
+  for (int m = 0; m <= mmax; ++m) {
+    for (int odd = 0; odd < 2; ++odd) {
+      const int mi = 2 * m + odd;
+      const int32_t nk = lmax - m - odd >= 0 ? (lmax - m - odd) / 2 + 1 : 0;
+      const int32_t *ks = kstart.data() + (size_t)mi * ni;
+      DevMatrix M{};
+      M.m = m;
+      M.odd = odd;
+      M.nk = nk;
+      M.ncols = ni;
+      M.nlevels = 0;
+      M.dblock_begin = (int32_t)P.dblocks.size();
+      M.level_begin = (int32_t)P.levels.size();
+      M.root_rows = ni;
+      M.xrow = -1;
+      DevDBlock D{};
+      D.row_start = 0;
+      D.nrows = nk;
+      D.ncols = ni;
+      D.out_row = 0;
+      D.strip_begin = (int32_t)P.strips.size();
+      D.aux = -1;
+      const int32_t dblock = (int32_t)P.dblocks.size();
+      std::vector<int32_t> rm(2 * (size_t)ni);
+      int64_t nnz = 0;
+      double cost = 0.0;
+      if (nk <= 4) {
+        // the whole block dense, nk x ni column-major
+        const int64_t data = zeros((size_t)nk * ni);
+        P.strips.push_back(DevStrip{0, 0, ni, 0, dblock, 0, data});
+        for (int c = 0; c < ni; ++c) {
+          const int32_t k0 = std::min(ks[c], nk);
+          fill[(size_t)mi * ni + c] = DevDenseFill{data + (int64_t)c * nk + k0, 1, nk - k0};
+          rm[2 * c] = D.strip_begin;
+          rm[2 * c + 1] = c;
+          nnz += nk - k0;
+        }
+        P.dense_elems += (int64_t)nk * ni;
+        cost += (double)nk * ni;
+      } else {
+        std::vector<double> aux(3 * (size_t)(nk - 2));
+        for (int32_t k = 2; k < nk; ++k)
+          rec_abg(m, m + odd, k, &aux[3 * (k - 2)], &aux[3 * (k - 2) + 1], &aux[3 * (k - 2) + 2]);
+        D.aux = (int64_t)append_f64(P.f64, (const char *)aux.data(), aux.size());
+        P.aux_values += (int64_t)aux.size();
+        // one strip per run of columns with the same first row
+        for (int c0 = 0; c0 < ni;) {
+          int c1 = c0 + 1;
+          while (c1 < ni && ks[c1] == ks[c0]) ++c1;
+          const int32_t rs = std::min(ks[c0], nk), nks = nk - rs, nx = c1 - c0;
+          DevStrip S{rs, c0, c1, 0, dblock, 0, 0};
+          if (nks > 4) {
+            S.kind = 1;
+            S.data = zeros(3 * (size_t)nx);
+            for (int c = c0; c < c1; ++c) {
+              P.f64[S.data + (c - c0)] = z[c] * z[c];
+              fill[(size_t)mi * ni + c] = DevDenseFill{S.data + nx + (c - c0), nx, 2};
+            }
+            P.rec_elems += (int64_t)nks * nx;
+            P.rec_columns += nx;
+            cost += 2.5 * nks * nx;
+          } else if (nks > 0) {
+            S.data = zeros((size_t)nks * nx);
+            for (int c = c0; c < c1; ++c)
+              fill[(size_t)mi * ni + c] = DevDenseFill{S.data + (int64_t)(c - c0) * nks, 1, nks};
+            P.dense_elems += (int64_t)nks * nx;
+            cost += (double)nks * nx;
+          }
+          for (int c = c0; c < c1; ++c) {
+            rm[2 * c] = (int32_t)P.strips.size();
+            rm[2 * c + 1] = c - c0;
+          }
+          nnz += (int64_t)nks * nx;
+          P.strips.push_back(S);
+          c0 = c1;
+        }
+      }
+      D.strip_end = (int32_t)P.strips.size();
+      P.dblocks.push_back(D);
+      M.dblock_end = (int32_t)P.dblocks.size();
+      M.root_map = (int64_t)append_i32(P.i32, rm);
+      M.cost = cost;
+      P.element_count[mi] = nnz;
+      P.mats.push_back(M);
+    }
+  }
+  P.max_rows = 0;
   return true;
 }
 

@@ -77,6 +77,17 @@ bool build_fast_path(HostProgram &P, std::string &err);
 // DevMatrix whose root buffer rows the caller provides.
 bool compile_butterfly_tree(const char *data, size_t len, HostProgram &P, std::string &err);
 
+// Ring-pair colatitude data of HEALPix (pair 0 = equator): z = cos(theta)
+// of the northern ring of every pair (src/wavemoth.c:1199-1232 geometry).
+std::vector<double> ring_pair_z(int nside);
+
+// Dense-recurrence program (no butterfly): every (m, parity) a depth-0
+// matrix with one block over all rings, column r starting at row
+// kstart[(2m + parity) ni + r]; the stored seed values are left zero and
+// listed in `fill` for the device (launch_dense_fill).
+bool build_dense_program(int nside, int lmax, int mmax, const std::vector<int32_t> &kstart, HostProgram &P,
+                         std::vector<DevDenseFill> &fill, std::string &err);
+
 // Parses a rev1 file image.  nside_expect < 0 accepts any nside.
 bool compile_resource(const char *data, size_t len, int nside_expect, int lmax_expect,
                       int mmax_expect, HostProgram &P, std::string &err);

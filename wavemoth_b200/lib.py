@@ -18,6 +18,7 @@ WAVEMOTH_NO_RESOURCE_COPY = 0x10
 WAVEMOTH_DEVICE_POINTERS = 0x100
 WAVEMOTH_PRECISION_SPLIT = 0x200
 WAVEMOTH_SPLIT_GENERATE = 0x400
+WAVEMOTH_DENSE = 0x800
 # precision= of the plans: FP64 tensor cores, or the split int8 path with the
 # residual P sliced once per plan ("split") or generated at every call
 # ("split-generate", less device memory)

@@ -10,7 +10,8 @@ import os
 import torch
 
 from . import _native
-from .lib import PRECISION_FLAGS, WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WavemothError, last_error
+from .lib import (PRECISION_FLAGS, WAVEMOTH_DENSE, WAVEMOTH_DEVICE_POINTERS, WAVEMOTH_MMAJOR, WavemothError,
+                  last_error)
 
 
 class Transform:
@@ -20,7 +21,10 @@ class Transform:
     FP64 ('split-generate': the residual P regenerated at every call instead
     of held sliced in device memory)."""
 
-    def __init__(self, resource_file, nside, lmax, nmaps=1, precision="double"):
+    def __init__(self, resource_file, nside, lmax, nmaps=1, precision="double", dense=False):
+        """dense=True: no butterfly file (resource_file may be None); every
+        (m, parity) block is one three-term recurrence over all rings,
+        seeded by the device's FP64 Legendre generator."""
         if not torch.cuda.is_available():
             raise RuntimeError("wavemoth_b200.Transform needs a CUDA device")
         self.nside, self.lmax, self.nmaps = nside, lmax, nmaps
@@ -30,10 +34,10 @@ class Transform:
         if precision not in PRECISION_FLAGS:
             raise ValueError("precision must be one of %s" % ", ".join(PRECISION_FLAGS))
         self.precision = precision
-        flags = WAVEMOTH_DEVICE_POINTERS | PRECISION_FLAGS[precision]
+        flags = WAVEMOTH_DEVICE_POINTERS | PRECISION_FLAGS[precision] | (WAVEMOTH_DENSE if dense else 0)
         lib = _native.lib()
-        p = lib.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR,
-                                         flags, os.fsencode(resource_file))
+        p = lib.wavemoth_plan_to_healpix(nside, lmax, lmax, nmaps, 1, None, None, WAVEMOTH_MMAJOR, flags,
+                                         os.fsencode(resource_file) if resource_file else None)
         if not p:
             raise WavemothError("plan creation failed: " + last_error())
         self._plan = p
