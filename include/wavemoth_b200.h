@@ -145,6 +145,37 @@ int64_t wavemoth_plan_image_bytes(wavemoth_plan plan);
    exercise allocation-failure handling without exhausting the GPU. */
 void wavemoth_set_device_memory_cap(int64_t bytes);
 
+/* ---- m-sharded transforms over several GPUs (one process per GPU) ----
+   Part `part` of `nparts` (every process makes the same call with its own
+   part): the Legendre step for a contiguous range of m (ranges balanced by
+   the matrices' estimated work) and the ring FFTs for a contiguous range of
+   ring pairs (balanced by pixels), with one all-to-all of q between them.
+   Device pointers, caller streams; the exchange itself is the caller's
+   (NCCL all-to-all; wavemoth_b200.shard.ShardedTransform does it with
+   torch.distributed).  Buffers, with nvecs = 2 nmaps, R_k = ring pairs and
+   M_k = m values of part k, this part p:
+     q_send (alm2map) / q_recv (map2alm): Legendre side,
+         [ring 0 .. 2 Nside)[m in M_p][parity][nvecs];
+     q_recv (alm2map) / q_send (map2alm): exchange side,
+         [part k][ring in R_p][m in M_k][parity][nvecs];
+     q_ring: ring side scratch, [ring in R_p][m 0 .. mmax][parity][nvecs].
+   alm2map: legendre (alm -> q_send), all-to-all (q_send block of part k =
+   its rings, in order), rings (q_recv -> the map's pixels of R_p).
+   map2alm: rings (map -> q_send, block of part k = its m), all-to-all,
+   legendre (q_recv -> alm rows of M_p).  New: the reference splits m over
+   threads of one host (src/wavemoth.c:496-552), not over devices. */
+wavemoth_plan wavemoth_plan_shard(int Nside, int lmax, int mmax, int nmaps, unsigned flags,
+                                  char *resource_filename, int nparts, int part);
+/* m_bounds[k] .. m_bounds[k + 1] and ring_bounds[k] .. ring_bounds[k + 1]
+   are part k's ranges (nparts + 1 entries each). */
+int wavemoth_shard_layout(wavemoth_plan plan, int64_t *m_bounds, int64_t *ring_bounds);
+int wavemoth_shard_alm2map_legendre(wavemoth_plan plan, const double *alm, double *q_send, void *stream);
+int wavemoth_shard_alm2map_rings(wavemoth_plan plan, const double *q_recv, double *q_ring, double *map,
+                                 void *stream);
+int wavemoth_shard_map2alm_rings(wavemoth_plan plan, const double *map, double *q_ring, double *q_send,
+                                 void *stream);
+int wavemoth_shard_map2alm_legendre(wavemoth_plan plan, const double *q_recv, double *alm, void *stream);
+
 /* Quadrature weights of the analysis direction: weights[r] (r = 0 .. 2 Nside
    - 1, ring pairs from the equator; positive) multiplies the pixels of the
    rings mid - r and mid + r in map2alm, a_lm = 4 pi / Npix sum_p w_r(p) f_p

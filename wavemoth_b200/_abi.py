@@ -43,6 +43,12 @@ SIGNATURES = {
     "wavemoth_plan_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_int64]),
     "wavemoth_execute_adjoint": (None, [_vp]),
     "wavemoth_plan_set_ring_weights": (ctypes.c_int, [_vp, _dp]),
+    "wavemoth_plan_shard": (_vp, [ctypes.c_int] * 4 + [ctypes.c_uint, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "wavemoth_shard_layout": (ctypes.c_int, [_vp, _vp, _vp]),
+    "wavemoth_shard_alm2map_legendre": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "wavemoth_shard_alm2map_rings": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "wavemoth_shard_map2alm_rings": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "wavemoth_shard_map2alm_legendre": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_map2alm_iterative_device": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     # kernel-level hooks (src/legendre_transform.h, src/butterfly.h.in)
     "wavemoth_legendre_transform_auxdata": (None, [_sz, _sz, _sz, _dp]),

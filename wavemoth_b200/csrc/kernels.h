@@ -191,6 +191,12 @@ cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
 // map2alm between the transforms
 cudaError_t launch_residual(const double *a, const double *b, double *y, int64_t n, cudaStream_t st);
 cudaError_t launch_accumulate(const double *x, double *y, int64_t n, cudaStream_t st);
+// m-sharded plans: moves the 2 nvecs doubles of every (ring of this part,
+// m) between the ring-side q (row (ring (mmax + 1) + m) 2 + parity, rings
+// counted from the part's first) and the exchange buffer (row pair of m at
+// tab[2m] + ring tab[2m + 1] doubles); gather 1: exchange -> ring side.
+cudaError_t launch_shard_exchange(const int64_t *tab, int64_t nrings, int32_t mcount, int32_t nvecs,
+                                  const double *src, double *dst, int gather, cudaStream_t st);
 cudaError_t launch_ring_analysis(const RingParams &prm, cudaStream_t st);
 cudaError_t launch_ring_setup(const RingParams &prm, double *twiddles, double *filters,
                               double *aux, double2 *phases, cudaStream_t st);

@@ -770,6 +770,7 @@ bool build_fast_path(HostProgram &P, std::string &err) {
     DevMatrix &M = P.mats[mi];
     M.fast = 0;
     M.xrow = -1;
+    if (P.shard_m1 >= 0 && (M.m < P.shard_m0 || M.m >= P.shard_m1)) continue;  // another shard's
     const int nblk = M.dblock_end - M.dblock_begin;
     bool ok = M.nk > 0 && (M.nlevels == 0 || M.nlevels == 1);
     if (ok && M.nlevels == 0) ok = (nblk == 1);

@@ -10,6 +10,9 @@ namespace wm {
 
 struct HostProgram {
   int nside = 0, lmax = 0, mmax = 0;
+  // m-sharded plans: the matrices of m in [shard_m0, shard_m1) are this
+  // plan's (shard_m1 < 0: all), and its q holds only those m (q_row)
+  int32_t shard_m0 = 0, shard_m1 = -1;
   int32_t max_rows = 0;                 // largest intermediate buffer over all matrices
   std::vector<DevMatrix> mats;          // (m, odd) in file order: index 2m + odd
   std::vector<DevDBlock> dblocks;
@@ -64,7 +67,12 @@ struct HostProgram {
 inline int64_t q_row(int mmax, int m, int odd, int64_t ring) {
   return (ring * (mmax + 1) + m) * 2 + odd;
 }
-inline int64_t q_row(const HostProgram &P, int m, int odd, int64_t ring) { return q_row(P.mmax, m, odd, ring); }
+inline int64_t q_row(const HostProgram &P, int m, int odd, int64_t ring) {
+  if (P.shard_m1 < 0) return q_row(P.mmax, m, odd, ring);
+  // a shard's q holds rows of its own m only: ring stride 2 (m1 - m0); the
+  // row index keeps m itself, the buffer's origin is moved back by 2 m0 rows
+  return (ring * (P.shard_m1 - P.shard_m0) + m) * 2 + odd;
+}
 
 // Streamed split GEMM launches.
 enum : int { kStreamResA2M = 0, kStreamResM2A = 1, kStreamLevelA2M = 2, kStreamLevelM2A = 3 };

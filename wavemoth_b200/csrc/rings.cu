@@ -755,6 +755,31 @@ __global__ void k_accumulate(const double *__restrict__ x, double *__restrict__ 
     y[i] += x[i];
 }
 
+// One warp per (ring, m) row pair: 2 nvecs doubles between the ring-side q
+// and the exchange buffer.
+__global__ void k_shard_exchange(const int64_t *__restrict__ tab, int64_t nrings, int32_t mcount, int32_t nvecs,
+                                 const double *__restrict__ src, double *__restrict__ dst, int gather) {
+  const int lane = threadIdx.x & 31;
+  const int64_t n = nrings * mcount;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+       i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t rl = i / mcount, m = i % mcount;
+    const int64_t ring_off = i * 2 * nvecs, x_off = tab[2 * m] + rl * tab[2 * m + 1];
+    const double *s = src + (gather ? x_off : ring_off);
+    double *d = dst + (gather ? ring_off : x_off);
+    for (int v = lane; v < 2 * nvecs; v += 32) d[v] = s[v];
+  }
+}
+
+cudaError_t launch_shard_exchange(const int64_t *tab, int64_t nrings, int32_t mcount, int32_t nvecs,
+                                  const double *src, double *dst, int gather, cudaStream_t st) {
+  const int64_t n = nrings * mcount;
+  if (n <= 0) return cudaSuccess;
+  k_shard_exchange<<<(unsigned)std::min<int64_t>((n + 7) / 8, 8192), 256, 0, st>>>(tab, nrings, mcount, nvecs, src,
+                                                                                     dst, gather);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_residual(const double *a, const double *b, double *y, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   k_residual<<<(unsigned)std::min<int64_t>((n + 255) / 256, 8192), 256, 0, st>>>(a, b, y, n);
