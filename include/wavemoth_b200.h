@@ -145,6 +145,15 @@ int64_t wavemoth_plan_image_bytes(wavemoth_plan plan);
    exercise allocation-failure handling without exhausting the GPU. */
 void wavemoth_set_device_memory_cap(int64_t bytes);
 
+/* The Legendre phase alone on device buffers, q in this library's layout
+   (rows of 2 nmaps doubles, (m, parity) of ring pair r at row
+   (r (mmax + 1) + m) 2 + parity): q = Lambda a for every (m, parity)
+   (alm2map), a = Lambda^T q (map2alm; no 4 pi / Npix, which the ring
+   analysis applies).  The device-buffer analogue of
+   wavemoth_perform_legendre_transforms (src/wavemoth_private.h:132). */
+int wavemoth_legendre_alm2map_device(wavemoth_plan plan, const double *alm, double *q, void *stream);
+int wavemoth_legendre_map2alm_device(wavemoth_plan plan, const double *q, double *alm, void *stream);
+
 /* ---- m-sharded transforms over several GPUs (one process per GPU) ----
    Part `part` of `nparts` (every process makes the same call with its own
    part): the Legendre step for a contiguous range of m (ranges balanced by

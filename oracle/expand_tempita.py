@@ -56,18 +56,22 @@ def _list_zip(*args):
     return list(zip(*args))
 
 
-def main(src, dst):
+def main(src, dst, **params):
     tempita = _load_tempita()
     with open(src) as f:
         text = f.read()
     # The templates were written for Python 2, where zip() returns a list
     # that can be iterated more than once (src/butterfly.c.in:31-36 iterates
     # nvecs_instances once per scatter group).
-    out = tempita.sub(text, zip=_list_zip)
+    out = tempita.sub(text, zip=_list_zip, **params)
     with open(dst, "w") as f:
         f.write("/* generated from %s by oracle/expand_tempita.py */\n" % src)
         f.write(out)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1], sys.argv[2])
+    # template parameters as name=python-literal pairs (the instantiation
+    # arguments of wavemoth/cuda/legendre_transform.py:23-33 for the GPU kernel)
+    import ast
+    params = dict((k, ast.literal_eval(v)) for k, v in (a.split("=", 1) for a in sys.argv[3:]))
+    main(sys.argv[1], sys.argv[2], **params)

@@ -43,6 +43,8 @@ SIGNATURES = {
     "wavemoth_plan_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_int64]),
     "wavemoth_execute_adjoint": (None, [_vp]),
     "wavemoth_plan_set_ring_weights": (ctypes.c_int, [_vp, _dp]),
+    "wavemoth_legendre_alm2map_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "wavemoth_legendre_map2alm_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_plan_shard": (_vp, [ctypes.c_int] * 4 + [ctypes.c_uint, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "wavemoth_shard_layout": (ctypes.c_int, [_vp, _vp, _vp]),
     "wavemoth_shard_alm2map_legendre": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
