@@ -62,7 +62,12 @@ def parse():
                          "butterfly plans at each of --dense-nsides (lmax = 2 nside), both precisions")
     ap.add_argument("--dense-nsides", default="32,64,128,256,512")
     ap.add_argument("--requests", type=int, default=24)
-    ap.add_argument("--uneven-nsides", default="64,128,256,512")
+    ap.add_argument("--uneven-nsides", default="128,256,512,1024,2048")
+    ap.add_argument("--max-nside2048", type=int, default=1,
+                    help="uneven batch: at most this many nside 2048 requests (later such draws are "
+                         "drawn again from the other nsides), so that the batch fits one GPU")
+    ap.add_argument("--schedule-cache", default=None,
+                    help="batch schedule cache (JSON); default a fresh file, so the search runs")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the comparison of maps 0-3 with the reference's own C alm2map "
                          "(run outside the timed region, rank 0 at N = 1)")
@@ -628,8 +633,12 @@ def run_uneven(a):
     nsides = [int(x) for x in a.uneven_nsides.split(",")]
     reqs, transforms = [], []
     total_maps = 0
+    n2048 = 0
     for i in range(a.requests):
         nside = int(rng.choice(nsides))
+        while nside >= 2048 and n2048 >= a.max_nside2048 and len(nsides) > 1:
+            nside = int(rng.choice([n for n in nsides if n < 2048]))
+        n2048 += nside >= 2048
         nmaps = int(rng.integers(1, 9))
         pa = types.SimpleNamespace(nside=nside, lmax=2 * nside, eps=a.eps, chunk=a.chunk, memop=a.memop,
                                    plan_dir=a.plan_dir)
@@ -664,9 +673,15 @@ def run_uneven(a):
             T.alm2map(alm, out=out)
 
     seq_ms = timed(sequential)
-    B = Batch(reqs)
-    width, _ = B.info()
+    cache = a.schedule_cache or tempfile.mktemp(prefix="wm_sched_", suffix=".json")
+    t0 = time.time()
+    B = Batch(reqs, cache=cache)
+    tune_s = time.time() - t0
+    width, sms, _ = B.schedule()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
     batch_ms = timed(B.execute)
+    clk = clocks.stop()
     for T in transforms:
         T.device_status()
     line = {"metric": "uneven batch alm2map maps/sec (split precision, one graph launch)",
@@ -674,7 +689,13 @@ def run_uneven(a):
             "warmup": a.warmup, "ms_per_step": batch_ms, "higher_is_better": True, "data": "synthetic",
             "config": {"workload": "uneven batch", "requests": a.requests, "nsides": nsides,
                        "lmax": "2 nside", "maps_per_request": "1-8 (seeded)", "total_maps": total_maps,
-                       "graph_branches": width, "l2": "flushed between timed launches"},
+                       "request_nsides": [T.nside for T in transforms],
+                       "request_maps": [T.nmaps for T in transforms],
+                       "request_precisions": [T.precision for T in transforms],
+                       "schedule": {"graph_branches": width, "sms_per_request": sms or "all",
+                                    "search_seconds": tune_s},
+                       "l2": "flushed between timed launches"},
+            "clocks": clk,
             "sequential": {"value": total_maps / (seq_ms / 1e3), "unit": "maps/s", "ms_per_step": seq_ms}}
     B.close()
     for T in transforms:

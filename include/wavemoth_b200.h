@@ -92,6 +92,17 @@ wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const
                                      int max_width, void *stream);
 /* One graph launch of every request of the batch on `stream`. */
 int wavemoth_batch_execute(wavemoth_batch batch, void *stream);
+
+/* wavemoth_batch_create with an explicit schedule search: schedules[2 k] =
+   parallel graph branches, schedules[2 k + 1] = SMs per request for the
+   persistent Legendre kernels (0: all; applied to every request when there
+   is more than one branch), k < nschedules.  Every schedule is captured and
+   timed, the fastest kept (one schedule: no timing).  The chosen one is
+   reported by wavemoth_batch_schedule. */
+wavemoth_batch wavemoth_batch_create_scheduled(int nreq, const wavemoth_plan *plans, const int *directions,
+                                               const double *const *inputs, double *const *outputs,
+                                               const int *schedules, int nschedules, void *stream);
+int wavemoth_batch_schedule(wavemoth_batch batch, int *width, int *sms, double *ms);
 /* The branch count the creation chose and its measured time per launch. */
 int wavemoth_batch_info(wavemoth_batch batch, int *width, double *ms);
 void wavemoth_batch_destroy(wavemoth_batch batch);
@@ -209,6 +220,12 @@ int wavemoth_map2alm_iterative_device(wavemoth_plan plan, const double *map, dou
    through wavemoth_plan_status.  New: the reference has no analysis
    direction (src/wavemoth.c:1271-1283 is synthesis only). */
 void wavemoth_execute_adjoint(wavemoth_plan plan);
+
+/* Caps the SMs the plan's persistent Legendre kernels (the tensor-core and
+   split GEMMs, which walk the plan's (m, parity) tile list) may occupy; 0
+   restores all.  Used by the batch scheduler so that concurrent requests
+   share the GPU; results do not depend on it. */
+int wavemoth_plan_set_grid_cap(wavemoth_plan plan, int sms);
 
 /* Test hook: how many times a wait of the streamed split-precision GEMM
    (wavemoth_execute_*_device with WAVEMOTH_PRECISION_SPLIT) polls its

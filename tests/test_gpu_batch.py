@@ -46,9 +46,15 @@ def test_uneven_batch_matches_single_calls():
         alms.append(a)
         reqs.append((T, direction, inp, out))
         singles.append(single)
-    B = Batch(reqs)
+    import tempfile
+    cache = tempfile.mktemp(prefix="wm_sched_", suffix=".json")
+    B = Batch(reqs, cache=cache)
     width, ms = B.info()
-    assert width in (1, 2, 4, 8) and ms > 0
+    assert width in (1, 2, 4, 8) and ms > 0 and not B.from_cache
+    # a batch of the same shape takes the cached schedule without a search
+    B2 = Batch(reqs, cache=cache)
+    assert B2.from_cache and B2.schedule()[:2] == B.schedule()[:2]
+    B2.close()
     for _ in range(2):
         for r in reqs:
             r[3].zero_()
@@ -76,3 +82,44 @@ def test_batch_rejects_shared_transform():
     with pytest.raises(ValueError):
         Batch([(T, "alm2map", a, m), (T, "alm2map", a, m)])
     T.close()
+
+
+def test_uneven_batch_with_nside512_against_reference():
+    """A batch holding an nside 512 (lmax 1024) split request next to smaller
+    ones: its maps against the reference's own C alm2map of the same alm on
+    the same plan file (<= 1e-9 max-abs over max-abs, the split bound), and
+    the FP64 request against the same at <= 1e-10."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("reference C library not built")
+    import os
+    import tempfile
+    from wavemoth_b200.batch import Batch
+    from wavemoth_b200.sht import Transform
+    workers = min(len(os.sched_getaffinity(0)), 32)
+    big = plan_file(512, 1024, 64, 1e-10, 20.0, workers=workers)
+    specs = [(512, 2, "split", big), (512, 1, "double", big), (128, 3, "split", None), (64, 5, "double", None)]
+    reqs, alms = [], []
+    for i, (nside, nmaps, prec, path) in enumerate(specs):
+        path = path or plan_file(nside, 2 * nside, 16, 1e-10, 20.0)
+        T = Transform(path, nside, 2 * nside, nmaps, precision=prec)
+        a = osht.random_alm(2 * nside, nmaps, seed=900 + i)
+        reqs.append((T, "alm2map", torch.from_numpy(a).cuda(),
+                     torch.empty((T.npix, nmaps), dtype=torch.float64, device="cuda")))
+        alms.append(a)
+    B = Batch(reqs, cache=tempfile.mktemp(prefix="wm_sched_", suffix=".json"))
+    B.execute()
+    torch.cuda.synchronize()
+    for (nside, nmaps, prec, path), (T, _, _, out), a in zip(specs, reqs, alms):
+        T.device_status()
+        if nside != 512:
+            continue
+        rp = ref.RefPlan(nside, 2 * nside, nmaps, big, nthreads=8)
+        rp.input[:] = a
+        want = rp.execute().copy()
+        rp.close()
+        tol = 1e-9 if prec == "split" else 1e-10
+        assert np.abs(out.cpu().numpy() - want).max() <= tol * np.abs(want).max()
+    B.close()
+    for r in reqs:
+        r[0].close()

@@ -30,6 +30,9 @@ SIGNATURES = {
     "wavemoth_batch_execute": (ctypes.c_int, [_vp, _vp]),
     "wavemoth_batch_info": (ctypes.c_int, [_vp, _vp, _vp]),
     "wavemoth_batch_destroy": (None, [_vp]),
+    "wavemoth_batch_create_scheduled": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "wavemoth_batch_schedule": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "wavemoth_plan_set_grid_cap": (ctypes.c_int, [_vp, ctypes.c_int]),
     "wavemoth_execute_alm2map_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_execute_map2alm_device": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "wavemoth_get_work": (ctypes.c_int, [_vp, _dp]),

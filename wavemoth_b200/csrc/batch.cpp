@@ -5,10 +5,13 @@
 // into one CUDA graph: they are ordered by their algorithmic work (Legendre
 // flops plus ring bytes, from wavemoth_plan_work) and assigned longest first
 // to the least-loaded of `width` parallel capture branches, so that small
-// transforms fill the SMs that large ones leave idle.  The width is
-// autotuned: a graph is built and timed for every width in {1, 2, 4, 8}
-// (at most the number of requests) and the fastest is kept.  Every
-// execute is then one cudaGraphLaunch.
+// transforms fill the SMs that large ones leave idle.  A schedule is the
+// branch count and, with more than one branch, the number of SMs every
+// request's persistent Legendre kernels may occupy (the CTAs that walk its
+// (m, parity) tile list; fewer leave room for the concurrent branches).
+// Schedules are autotuned: each candidate is captured, instantiated and
+// timed, and the fastest is kept (wavemoth_b200.batch caches the choice per
+// batch signature).  Every execute is then one cudaGraphLaunch.
 //
 // The plans' own buffers (q, X, operand slices) are shared by all calls on
 // one plan, so a batch must not hold two requests on the same plan.
@@ -38,6 +41,7 @@ struct _wavemoth_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int width = 0;
+  int sms = 0;  // SMs per request of the chosen schedule (0: all)
   double ms = 0.0;
 
   ~_wavemoth_batch() {
@@ -48,13 +52,24 @@ struct _wavemoth_batch {
 
 namespace {
 
+int capture_branches(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGraph_t *out);
+
 int cuda_err(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return 0;
   return wm::set_last_error(WAVEMOTH_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Captures the batch with `width` branches forked from `origin`.
-int capture(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGraph_t *out) {
+// Captures the batch with `width` branches forked from `origin`, every
+// request's persistent Legendre kernels capped at `sms` SMs (launch sizes
+// are fixed into the graph; the plans' caps are restored afterwards).
+int capture(_wavemoth_batch &B, int width, int sms, cudaStream_t origin, cudaGraph_t *out) {
+  for (const auto &r : B.reqs) wavemoth_plan_set_grid_cap(r.plan, width > 1 ? sms : 0);
+  const int rc = capture_branches(B, width, origin, out);
+  for (const auto &r : B.reqs) wavemoth_plan_set_grid_cap(r.plan, 0);
+  return rc;
+}
+
+int capture_branches(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGraph_t *out) {
   std::vector<cudaStream_t> br(width, nullptr);
   std::vector<cudaEvent_t> done(width, nullptr);
   cudaEvent_t fork = nullptr;
@@ -118,12 +133,14 @@ int time_graph(cudaGraphExec_t ex, cudaStream_t st, int reps, double *ms) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const int *directions,
-                                     const double *const *inputs, double *const *outputs, int max_width,
-                                     void *stream) {
-  if (nreq <= 0 || !plans || !directions || !inputs || !outputs) {
+// Validates the requests, estimates their costs and runs the schedule
+// search over `schedules` (pairs of branches, SMs per request).
+wavemoth_batch create_batch(int nreq, const wavemoth_plan *plans, const int *directions,
+                            const double *const *inputs, double *const *outputs,
+                            const std::vector<std::pair<int, int>> &schedules, void *stream) {
+  if (nreq <= 0 || !plans || !directions || !inputs || !outputs || schedules.empty()) {
     wm::set_last_error(WAVEMOTH_ERR_ARG, "invalid batch arguments");
     return nullptr;
   }
@@ -159,14 +176,14 @@ wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const
     delete B;
     return nullptr;
   }
-  const int wmax = std::max(1, std::min(std::min(nreq, 8), max_width > 0 ? max_width : 8));
-  for (int width = 1; width <= wmax; width *= 2) {
+  for (const auto &sc : schedules) {
+    const int width = std::max(1, std::min(sc.first, nreq)), sms = std::max(0, sc.second);
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ex = nullptr;
-    int rc = capture(*B, width, st, &g);
+    int rc = capture(*B, width, sms, st, &g);
     if (!rc) rc = cuda_err(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
     double ms = 0.0;
-    if (!rc) rc = time_graph(ex, st, 3, &ms);
+    if (!rc && schedules.size() > 1) rc = time_graph(ex, st, 3, &ms);
     if (rc) {
       if (ex) cudaGraphExecDestroy(ex);
       if (g) cudaGraphDestroy(g);
@@ -180,6 +197,7 @@ wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const
       B->exec = ex;
       B->graph = g;
       B->width = width;
+      B->sms = width > 1 ? sms : 0;
       B->ms = ms;
     } else {
       cudaGraphExecDestroy(ex);
@@ -189,6 +207,41 @@ wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const
   cudaStreamSynchronize(st);
   cudaStreamDestroy(st);
   return B;
+}
+
+}  // namespace
+
+extern "C" {
+
+wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const int *directions,
+                                     const double *const *inputs, double *const *outputs, int max_width,
+                                     void *stream) {
+  // branch counts 1, 2, 4, 8 (up to max_width and the request count), every
+  // request on all SMs
+  std::vector<std::pair<int, int>> sched;
+  const int wmax = std::max(1, std::min(std::min(nreq, 8), max_width > 0 ? max_width : 8));
+  for (int width = 1; width <= wmax; width *= 2) sched.push_back({width, 0});
+  return create_batch(nreq, plans, directions, inputs, outputs, sched, stream);
+}
+
+wavemoth_batch wavemoth_batch_create_scheduled(int nreq, const wavemoth_plan *plans, const int *directions,
+                                               const double *const *inputs, double *const *outputs,
+                                               const int *schedules, int nschedules, void *stream) {
+  if (!schedules || nschedules <= 0) {
+    wm::set_last_error(WAVEMOTH_ERR_ARG, "no schedules given");
+    return nullptr;
+  }
+  std::vector<std::pair<int, int>> sched;
+  for (int k = 0; k < nschedules; ++k) sched.push_back({schedules[2 * k], schedules[2 * k + 1]});
+  return create_batch(nreq, plans, directions, inputs, outputs, sched, stream);
+}
+
+int wavemoth_batch_schedule(wavemoth_batch batch, int *width, int *sms, double *ms) {
+  if (!batch) return wm::set_last_error(WAVEMOTH_ERR_ARG, "NULL batch");
+  if (width) *width = batch->width;
+  if (sms) *sms = batch->sms;
+  if (ms) *ms = batch->ms;
+  return 0;
 }
 
 int wavemoth_batch_execute(wavemoth_batch batch, void *stream) {
