@@ -198,37 +198,126 @@ class ClockSampler:
 
 # ------------------------------------------------------------ CPU baseline
 
+_REF_WORKER = {}
+
+
+def _ref_worker_init(nside, lmax, nmaps, path, threads, seed0):
+    """Pool worker: one reference plan of `threads` threads (a process of its
+    own: the reference's plan code is reliable with at most 8 threads, one
+    per presented NUMA node)."""
+    from oracle import ref
+    with ref.stdout_to_stderr():
+        rp = ref.RefPlan(nside, lmax, nmaps, path, nthreads=threads)
+    rp.input[:] = synthetic_alm(lmax, nmaps, seed0)
+    _REF_WORKER["rp"] = rp
+
+
+def _ref_worker_run(what):
+    rp = _REF_WORKER["rp"]
+    t0 = time.perf_counter()
+    if what == "legendre":
+        rp.perform_legendre_transforms()
+    else:
+        rp.execute()
+    return time.perf_counter() - t0
+
+
 class ReferenceRunner:
     """The reference's own C alm2map (oracle/_ref, built from its sources)
-    on the host cores, with as many threads as its plan code runs reliably
-    (one per presented NUMA node, at most 8).  The reference has no map2alm;
-    a round trip is costed as two alm2map executes (the adjoint performs the
-    same multiply-adds over the same compressed matrices)."""
+    on the host cores: the first plan in this process (maps 0-3, the
+    parity sample) and, to use every core, further independent plans in
+    worker processes (spawned), each with 8 threads (its plan code runs
+    reliably with at most one thread per presented NUMA node, at most 8).
+    A step runs every plan's execute at once; the rate is all plans' maps
+    over the wall time.  The reference has no map2alm; a round trip is
+    costed as two alm2map executes (the adjoint performs the same
+    multiply-adds over the same compressed matrices)."""
 
-    def __init__(self, a, path, nmaps=4):
+    def __init__(self, a, path, nmaps=4, all_cores=True):
         from oracle import ref
         self.nmaps = nmaps
-        self.threads = max(1, min(ref.MAX_THREADS, len(os.sched_getaffinity(0))))
+        cores = len(os.sched_getaffinity(0))
+        self.threads = max(1, min(ref.MAX_THREADS, cores))
         with ref.stdout_to_stderr():
             self.rp = ref.RefPlan(a.nside, a.lmax, nmaps, path, nthreads=self.threads)
         self.rp.input[:] = synthetic_alm(a.lmax, nmaps, 1000)
+        self.extra = max(0, cores // self.threads - 1) if all_cores else 0
+        self.pool = None
+        if self.extra:
+            import multiprocessing as mp
+            self.pool = mp.get_context("spawn").Pool(
+                self.extra, initializer=_ref_worker_init,
+                initargs=(a.nside, a.lmax, nmaps, path, self.threads, 2000))
 
-    def execute(self):
+    def _run(self, what):
         t0 = time.perf_counter()
-        self.rp.execute()
+        pending = self.pool.map_async(_ref_worker_run, [what] * self.extra) if self.pool else None
+        if what == "legendre":
+            self.rp.perform_legendre_transforms()
+        else:
+            self.rp.execute()
+        if pending is not None:
+            pending.get()
         return time.perf_counter() - t0
 
+    def execute(self):
+        return self._run("execute")
+
+    def legendre(self):
+        return self._run("legendre")
+
+    @property
+    def plans(self):
+        return 1 + self.extra
+
     def rate(self, t):
-        return self.nmaps / (2.0 * t)
+        return self.plans * self.nmaps / (2.0 * t)
 
     def describe(self, n):
         return ("reference C alm2map (wavemoth_execute; FFT through the oracle's shim, not "
-                "FFTW), %d maps per execute, %d thread(s); best of %d executes after warm-up; "
-                "round trip costed as 2 alm2map (the reference has no map2alm)"
-                % (self.nmaps, self.threads, n))
+                "FFTW), %d plan(s) of %d maps and %d thread(s) running at once (%d cores); best of "
+                "%d steps after warm-up; round trip costed as 2 alm2map (the reference has no map2alm)"
+                % (self.plans, self.nmaps, self.threads, self.plans * self.threads, n))
 
     def close(self):
         self.rp.close()
+        if self.pool is not None:
+            self.pool.close()
+            self.pool.join()
+            self.pool = None
+
+
+def map2alm_restatement_rate(a, path, seconds):
+    """map2alm on the host: the reference has none, so this times the
+    oracle's FP64 restatement (numpy FFT per ring, butterfly transposed
+    applies of the same plan file) on one map, over the m values it reaches
+    in `seconds` (every step-th m), scaled to all m by their Legendre
+    elements.  One thread (numpy)."""
+    from oracle import sht as osht
+    f = osht.Rev1File(path)
+    npix = 12 * a.nside * a.nside
+    maps = np.random.default_rng(5).standard_normal((npix, 1))
+    t0 = time.perf_counter()
+    work = osht.forward_ffts(maps, a.nside, a.lmax)
+    t_fft = time.perf_counter() - t0
+    step = max(1, (a.lmax + 1) // 64)
+    done_elems, t_leg = 0, 0.0
+    total = sum(a.lmax - m + 1 for m in range(a.lmax + 1))
+    for m in range(0, a.lmax + 1, step):
+        t1 = time.perf_counter()
+        for odd in (0, 1):
+            mat = f.matrix(m, odd)
+            nk = max(0, (a.lmax - m - odd) // 2 + 1)
+            if mat is not None and nk:
+                mat.apply(np.ascontiguousarray(work[m, odd]).view(np.float64).reshape(2 * a.nside, 2), nk)
+        t_leg += time.perf_counter() - t1
+        done_elems += a.lmax - m + 1
+        if t_fft + t_leg > seconds:
+            break
+    t_full = t_fft + t_leg * total / max(done_elems, 1)
+    return {"value": 1.0 / t_full, "unit": "maps/s (map2alm only)", "cores": 1, "kind": "port",
+            "sample": "oracle restatement (numpy FFT + butterfly transposed applies of the same plan "
+                      "file), 1 map; Legendre timed over %d elements of %d and scaled" % (done_elems, total)}
 
 
 def reference_rate(a, path, seconds, runner=None):
@@ -241,8 +330,12 @@ def reference_rate(a, path, seconds, runner=None):
         if time.time() > t_end:
             break
     best = min(times)
-    out = {"value": r.rate(best), "unit": "maps/s", "cores": r.threads, "kind": "reference",
-           "sample": r.describe(len(times)), "seconds_per_execute": best}
+    leg = min(r.legendre() for _ in range(3))
+    out = {"value": r.rate(best), "unit": "maps/s", "cores": r.threads * r.plans, "kind": "reference",
+           "sample": r.describe(len(times)), "seconds_per_execute": best,
+           "legendre_phase": {"value": r.plans * r.nmaps / leg, "unit": "maps/s (alm2map Legendre phase "
+                              "only, wavemoth_perform_legendre_transforms: shbench -F)",
+                              "seconds_per_call": leg}}
     r.close()
     return out
 
@@ -542,7 +635,7 @@ def run_b200(a):
     cpu, parity, runner = None, None, None
     if rank == 0 and world == 1 and not (a.no_cpu_baseline and a.no_parity):
         try:
-            runner = ReferenceRunner(a, path)
+            runner = ReferenceRunner(a, path, all_cores=not a.no_cpu_baseline)
         except Exception as ex:  # reported, never fatal for the GPU number
             err = str(ex)[:200]
             parity = {"unavailable": "reference C library: " + err}
@@ -554,6 +647,10 @@ def run_b200(a):
             cpu = reference_rate(a, path, a.cpu_baseline_seconds, runner=runner)
         except Exception as ex:
             cpu = {"value": None, "unit": "maps/s", "error": str(ex)[:200]}
+        try:
+            cpu["map2alm_restatement"] = map2alm_restatement_rate(a, path, a.cpu_baseline_seconds)
+        except Exception as ex:
+            cpu["map2alm_restatement"] = {"error": str(ex)[:200]}
     elif runner is not None:
         runner.close()
     if parity is not None and "adjoint" in head:
@@ -598,8 +695,8 @@ def run_reference(a):
         r.execute()
     times = [r.execute() for _ in range(a.steps)]
     total = sum(times)
-    value = r.nmaps * len(times) / (2.0 * total)
-    cpu = {"value": value, "unit": "maps/s", "cores": r.threads, "kind": "reference",
+    value = r.plans * r.nmaps * len(times) / (2.0 * total)
+    cpu = {"value": value, "unit": "maps/s", "cores": r.threads * r.plans, "kind": "reference",
            "sample": r.describe(len(times))}
     r.close()
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "maps/s",
@@ -608,7 +705,7 @@ def run_reference(a):
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded N(0,1)(l+1)^-1 alm)",
            "config": {"workload": "alm2map+map2alm round trip, nside %d, lmax=mmax %d; each step "
-                                  "a sample of %d maps" % (a.nside, a.lmax, r.nmaps),
+                                  "a sample of %d maps" % (a.nside, a.lmax, r.plans * r.nmaps),
                       "nside": a.nside, "lmax": a.lmax},
            "cpu_baseline": cpu,
            "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0,
