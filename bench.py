@@ -493,12 +493,15 @@ def run_b200(a):
             step_p(alm)
         torch.cuda.synchronize()
         barrier()
+        TP.timing(1)
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record()
         for _ in range(a.steps):
             step_p(alm)
         p1.record()
         torch.cuda.synchronize()
+        pkt = TP.timing(2)
+        TP.timing(0)
         pms = 1e3 * reduce_max_seconds(p0.elapsed_time(p1) / 1e3, dist if world > 1 else None)
         step(alm)
         torch.cuda.synchronize()
@@ -513,6 +516,15 @@ def run_b200(a):
                  "max_rel_error_alm_round_trip": maxrel(alm_out, alm_p),
                  "error_definition": "max |split - plain FP64| / max |plain FP64| over the alm2map "
                                      "output and over the alm2map+map2alm output, same inputs"}
+        # the plain path's FP64 tensor-core Legendre phases against DGEMM
+        fp64_peak = fp64_peak_tflops(torch)
+        plain["legendre_fp64"] = {}
+        for k in ("legendre_alm2map", "legendre_map2alm"):
+            lms = pkt["ms"][k] / max(pkt["launches"][k], 1)
+            ach = work["legendre_flops"] / (lms / 1e3) / 1e12
+            plain["legendre_fp64"][k] = {"ms_per_launch": lms, "achieved_tflops": ach, "peak_tflops": fp64_peak,
+                                         "frac": ach / fp64_peak}
+        plain["legendre_fp64"]["peak_source"] = "cuBLAS DGEMM 8192^3 measured by bench.py on this GPU"
         head["plain"] = maps_p[:, :4].cpu().numpy()
         head["adjoint"] = {"plain": adjoint_identity(torch, TP, alm, maps_p, T.npix),
                            "split": adjoint_identity(torch, T, alm, maps, T.npix)}
@@ -627,6 +639,21 @@ def run_b200(a):
                     "algorithmic_bytes_per_launch": work["ring_bytes"]}
     roofline["kernel_ms_per_launch"] = kms
     roofline["kernel_time_share"] = share
+    # the ring kernels against FP64 as well: measured with every global load
+    # and store of a ring kernel removed they keep ~80% of their time, so
+    # their bound is arithmetic (FFT passes, folds), not HBM
+    from wavemoth_b200.healpix import get_ring_pixel_counts
+    n = get_ring_pixel_counts(a.nside).astype(np.float64)
+    ring_flops = float(np.sum(2.5 * n * np.log2(n))) * a.nmaps
+    fp64_ring_peak = fp64_peak_tflops(torch)
+    roofline["ring_fp64_view"] = {
+        k: {"achieved_tflops": ring_flops / (kms[k] / 1e3) / 1e12, "peak_tflops": fp64_ring_peak,
+            "frac": ring_flops / (kms[k] / 1e3) / 1e12 / fp64_ring_peak,
+            "hbm_frac": work["ring_bytes"] / (kms[k] / 1e3) / 1e9 / peak_hbm}
+        for k in ("ring_synthesis", "ring_analysis")}
+    roofline["ring_fp64_view"]["flops_per_launch"] = ring_flops
+    roofline["ring_fp64_view"]["what"] = ("nominal real-FFT flops, 2.5 n log2 n per ring of n pixels per map, "
+                                          "over the kernel time; peak cuBLAS DGEMM 8192^3 on this GPU")
 
     # ---------------- parity and CPU baseline (rank 0, N = 1) ----------------
     # maps 0-3 of the batch (seeds 1000-1003) against the reference's own C
