@@ -327,7 +327,15 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
     return base[row * rstride + v];
   };
   double mx = 0.0;
-  for (int k = qtr; k < K; k += 4) mx = fmax(mx, fabs(entry(k)));
+  // group columns (K up to the ring count, rows gathered through the column
+  // table) keep sixteen rows' loads in flight per thread; the short ranges
+  // of the other modes run faster with the compiler's own unrolling
+  if constexpr (kMode == 1) {
+#pragma unroll 16
+    for (int k = qtr; k < K; k += 4) mx = fmax(mx, fabs(entry(k)));
+  } else {
+    for (int k = qtr; k < K; k += 4) mx = fmax(mx, fabs(entry(k)));
+  }
   red[qtr][v] = mx;
   __syncthreads();
   if (qtr == 0) {
@@ -338,7 +346,7 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
   __syncthreads();
   const double s = sc[v].x;
   int8_t *pl = p.planes + plane * (int64_t)kSplitPlane;
-  for (int ch = 0; ch < nch; ++ch) {
+  auto slice_chunk = [&](int ch) {
     uint32_t w[kSplitSlices][4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -352,6 +360,12 @@ __device__ void slice_operand(const SplitParams &p, int gi) {
 #pragma unroll
     for (int sl = 0; sl < kSplitSlices; ++sl)
       *reinterpret_cast<uint4 *>(dst + sl * kSliceB) = make_uint4(w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
+  };
+  if constexpr (kMode == 1) {
+#pragma unroll 2
+    for (int ch = 0; ch < nch; ++ch) slice_chunk(ch);
+  } else {
+    for (int ch = 0; ch < nch; ++ch) slice_chunk(ch);
   }
 }
 
