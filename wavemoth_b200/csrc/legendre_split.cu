@@ -829,8 +829,8 @@ __global__ void __launch_bounds__(kSplitM) k_level_slices(SplitParams p) {
   }
 }
 
-// One-dimensional bulk copy (TMA, no multicast) completing on `bar`, and the
-// arrival that announces its bytes.
+// One-dimensional bulk copy (TMA) into this CTA's own shared memory,
+// completing on `bar`, and the arrival that announces its bytes.
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -849,7 +849,7 @@ __device__ __forceinline__ void expect_tx(uint64_t *bar, uint32_t bytes) {
 // kernel serves the residual and level products of both directions.
 // Warp roles (one CTA per SM, persistent over the tile list):
 //   warp 0   one thread loads chunk after chunk with 1D bulk copies (TMA,
-//            no multicast) into kStreamStages stages, running ahead into the
+//            each into this CTA only) into kStreamStages stages, running ahead into the
 //            next tile while the current one drains;
 //   warp 1   one thread issues the nine MMAs per K step of 32 and commits
 //            each stage back to the loader, the finished tile to the
