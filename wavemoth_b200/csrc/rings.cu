@@ -15,9 +15,13 @@
 // and the analysis r2c uses the mirror identity.
 //
 // Length-N transforms, in place in shared memory, as passes of radix 16 (and
-// one pass of radix 2, 4 or 8 when log2 of the length is not a multiple of
-// 4); a pass loads 16 points per butterfly into registers and runs four
-// radix-2 stages there:
+// one last decimation-in-frequency pass of radix 2, 4 or 8 when log2 of the
+// length is not a multiple of 4); a pass loads 16 points per butterfly into
+// registers and runs four radix-2 stages there.  The first radix-16 pass of
+// a decimation in frequency leaves 16 independent blocks per lane; each of
+// the CTA's 16 warps owns one and runs the later passes (the earlier ones of
+// a decimation in time) on it alone, with warp barriers in place of CTA
+// barriers:
 //   * N a power of two (every belt ring): synthesis by decimation in
 //     frequency (natural order in, bit-reversed out), analysis by decimation
 //     in time (bit-reversed in, natural out).  Z is formed in natural order
@@ -65,6 +69,8 @@ namespace {
 
 constexpr int kRadixLog = 4;           // largest pass radix 2^kRadixLog
 constexpr int kRingThreads = 512;      // 16 points per thread of a kRingBufferCplx buffer
+constexpr int kRingWarps = kRingThreads / 32;
+static_assert(kRingWarps == 16, "warp-local passes give each of 16 warps the blocks of a radix-16 pass");
 constexpr int kPhaseLo = kRingPhaseLo;  // e^{i m phi0} = hi[m / 64] * lo[m % 64]
 
 struct cplx {
@@ -199,16 +205,41 @@ struct FftCtx {
   int lg;
 };
 
+// Butterflies of a pass, `body(b, g)` for butterfly b (per lane) of lane g.
+// wl == 0: all the CTA's threads over all butterflies, then a CTA barrier.
+// wl > 0: warp w alone runs the butterflies inside its own blocks of 2^wl
+// points of every lane, then a warp barrier -- for the passes after the
+// first radix-16 pass of a decimation in frequency (and before the last of
+// a decimation in time), whose blocks nest in those the warp owns, so that
+// warps run these passes without waiting for one another.
+template <int LR, class BodyF>
+__device__ __forceinline__ void for_butterflies(const FftCtx &f, int wl, BodyF body) {
+  const int gm = (1 << f.lg) - 1;
+  if (wl == 0) {
+    const int nbf = (f.M >> LR) << f.lg;
+    for (int t = threadIdx.x; t < nbf; t += blockDim.x) body(t >> f.lg, t & gm);
+    __syncthreads();
+  } else {
+    // warp w owns the blocks [w k, (w + 1) k): nblk >= 16 blocks (a power of
+    // two) over the CTA's 16 warps; its lanes run over (block, butterfly)
+    const int k = (f.M >> wl) / kRingWarps, warp = threadIdx.x >> 5;
+    const int lp = wl - LR + f.lg;  // log2 of the butterflies of one block, all lanes
+    for (int i = threadIdx.x & 31; i < (k << lp); i += 32) {
+      const int B = warp * k + (i >> lp), u = i & ((1 << lp) - 1);
+      body((B << (wl - LR)) + (u >> f.lg), u & gm);
+    }
+    __syncwarp();
+  }
+}
+
 // One in-place pass of radix R over the 2^lg interleaved sequences of length
 // M: butterfly b of lane g takes the points base + i q (q = len / R, len =
 // 2^lglen) of its block, through `load(index, g)` and `store(index, g, value)`.
 template <int R, int SIGN, bool DIF, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_pass(const FftCtx &f, int lglen, LoadF load, StoreF store) {
+__device__ __forceinline__ void fft_pass(const FftCtx &f, int lglen, int wl, LoadF load, StoreF store) {
   constexpr int LR = Log2<R>::v;
-  const int gm = (1 << f.lg) - 1, lq = lglen - LR;
-  const int nbf = (f.M >> LR) << f.lg;
-  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
-    const int g = t & gm, b = t >> f.lg;
+  const int lq = lglen - LR;
+  for_butterflies<LR>(f, wl, [&](int b, int g) {
     const int j = b & ((1 << lq) - 1), base = ((b >> lq) << lglen) + j;
     cplx A[LR];
     stage_twiddles<R, SIGN, DIF>(A, j, lglen, f.tw, f.lgtw);
@@ -219,22 +250,21 @@ __device__ __forceinline__ void fft_pass(const FftCtx &f, int lglen, LoadF load,
     else dit_regs<R, SIGN>(x, A);
 #pragma unroll
     for (int i = 0; i < R; ++i) store(base + (i << lq), g, x[i]);
-  }
-  __syncthreads();
+  });
 }
 
 template <int SIGN, bool DIF, class LoadF, class StoreF>
-__device__ __forceinline__ void fft_pass_r(const FftCtx &f, int R, int lglen, LoadF load, StoreF store) {
+__device__ __forceinline__ void fft_pass_r(const FftCtx &f, int R, int lglen, int wl, LoadF load, StoreF store) {
   switch (R) {
-    case 2: fft_pass<2, SIGN, DIF>(f, lglen, load, store); break;
-    case 4: fft_pass<4, SIGN, DIF>(f, lglen, load, store); break;
+    case 2: fft_pass<2, SIGN, DIF>(f, lglen, wl, load, store); break;
+    case 4: fft_pass<4, SIGN, DIF>(f, lglen, wl, load, store); break;
     case 8:
       if (kRadixLog > 3) {
-        fft_pass<8, SIGN, DIF>(f, lglen, load, store);
+        fft_pass<8, SIGN, DIF>(f, lglen, wl, load, store);
         break;
       }
       [[fallthrough]];
-    default: fft_pass<(1 << kRadixLog), SIGN, DIF>(f, lglen, load, store); break;
+    default: fft_pass<(1 << kRadixLog), SIGN, DIF>(f, lglen, wl, load, store); break;
   }
 }
 
@@ -244,15 +274,14 @@ __device__ __forceinline__ void fft_pass_r(const FftCtx &f, int R, int lglen, Lo
 // reflection F'(k) = conj F(-k)), inverse DIT stages.  Block offset 0: every
 // stage twiddle is 1.
 template <int R, class LoadF, class StoreF>
-__device__ __forceinline__ void bluestein_mid_r(const FftCtx &f, const cplx *F, int fsign, LoadF load,
+__device__ __forceinline__ void bluestein_mid_r(const FftCtx &f, const cplx *F, int fsign, int wl, LoadF load,
                                                 StoreF store) {
-  const int gm = (1 << f.lg) - 1, bitsM = ilog2(f.M);
-  const int nbf = (f.M / R) << f.lg;
+  const int bitsM = ilog2(f.M);
   cplx one[Log2<R>::v];
 #pragma unroll
   for (int s = 0; s < Log2<R>::v; ++s) one[s] = {1.0, 0.0};
-  for (int t = threadIdx.x; t < nbf; t += blockDim.x) {
-    const int g = t & gm, base = (t >> f.lg) * R;
+  for_butterflies<Log2<R>::v>(f, wl, [&](int b, int g) {
+    const int base = b * R;
     cplx x[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) x[i] = load(base + i, g);
@@ -273,41 +302,54 @@ __device__ __forceinline__ void bluestein_mid_r(const FftCtx &f, const cplx *F, 
     dit_regs<R, 1>(x, one);
 #pragma unroll
     for (int i = 0; i < R; ++i) store(base + i, g, x[i]);
-  }
-  __syncthreads();
+  });
 }
 
 template <class LoadF, class StoreF>
-__device__ __forceinline__ void bluestein_mid(const FftCtx &f, int R, const cplx *F, int fsign, LoadF load,
+__device__ __forceinline__ void bluestein_mid(const FftCtx &f, int R, const cplx *F, int fsign, int wl, LoadF load,
                                               StoreF store) {
   switch (R) {
-    case 2: bluestein_mid_r<2>(f, F, fsign, load, store); break;
-    case 4: bluestein_mid_r<4>(f, F, fsign, load, store); break;
+    case 2: bluestein_mid_r<2>(f, F, fsign, wl, load, store); break;
+    case 4: bluestein_mid_r<4>(f, F, fsign, wl, load, store); break;
     case 8:
       if (kRadixLog > 3) {
-        bluestein_mid_r<8>(f, F, fsign, load, store);
+        bluestein_mid_r<8>(f, F, fsign, wl, load, store);
         break;
       }
       [[fallthrough]];
-    default: bluestein_mid_r<(1 << kRadixLog)>(f, F, fsign, load, store); break;
+    default: bluestein_mid_r<(1 << kRadixLog)>(f, F, fsign, wl, load, store); break;
   }
 }
 
-// Pass radices of a length-M transform in DIF order: 2^(log2 M mod 4) (if
-// above 1) then 16s.  DIT runs them in reverse order.  Computed per pass
-// (no per-thread arrays, which would live in local memory).
+// Pass radices of a length-M transform in DIF order: the radix-16 passes
+// and one pass of radix 2^(log2 M mod 4) (if above 1), first or last.  DIT
+// runs them in reverse order.  Once the passes before p have cut every
+// lane into at least 16 blocks (one or more per warp of the CTA), pass p and
+// the later DIF passes (the earlier DIT passes) run warp-local on the blocks
+// of pass p0 (for_butterflies).  Computed per pass (no per-thread arrays,
+// which would live in local memory).
+template <bool kSmallFirst>
 struct Radices {
   int lgM;  // log2 M
-  int r0;   // log2 M mod 4: log2 of the radix of the first DIF pass, 0 if none
+  int r0;   // log2 M mod 4: log2 of the small radix, 0 if none
   int n;    // number of passes
   // radix of DIF pass p
-  __device__ __forceinline__ int r(int p) const { return (p == 0 && r0) ? 1 << r0 : 1 << kRadixLog; }
+  __device__ __forceinline__ int r(int p) const {
+    return (r0 && p == (kSmallFirst ? 0 : n - 1)) ? 1 << r0 : 1 << kRadixLog;
+  }
   // log2 of the block length of DIF pass p (the DIT pass mirroring it has the same)
-  __device__ __forceinline__ int lgl(int p) const { return p == 0 ? lgM : lgM - r0 - kRadixLog * (p - (r0 ? 1 : 0)); }
+  __device__ __forceinline__ int lgl(int p) const {
+    return lgM - kRadixLog * p + ((kSmallFirst && r0 && p > 0) ? kRadixLog - r0 : 0);
+  }
+  // first warp-local DIF pass: the first after a radix-16 pass
+  __device__ __forceinline__ int p0() const { return (kSmallFirst && r0) ? 2 : 1; }
+  // log2 of the per-lane block a warp owns in pass p (0: the whole CTA runs the pass)
+  __device__ __forceinline__ int wl(int p) const { return (p >= p0() && p < n) ? lgl(p0()) : 0; }
 };
 
-__device__ __forceinline__ Radices radices(int M) {
-  Radices s;
+template <bool kSmallFirst>
+__device__ __forceinline__ Radices<kSmallFirst> radices(int M) {
+  Radices<kSmallFirst> s;
   s.lgM = ilog2(M);
   s.r0 = s.lgM % kRadixLog;
   s.n = s.lgM / kRadixLog + (s.r0 ? 1 : 0);
@@ -452,7 +494,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
   // q rows are ring-major: (m, parity) of ring r at row (r (mmax + 1) + m) 2 + parity
   const int64_t half = p.nvecs, qstride = 2 * half;
   const double *qbase = p.q + (int64_t)c.ring * (p.mmax + 1) * qstride + 2 * c.map0;
-  const Radices rs = radices(M);
+  const auto rs = radices<false>(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = (c.pow2 ? 1.0 : 1.0 / (double)M) * p.map_scale;
@@ -538,23 +580,25 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
     };
     if (c.pow2) {
       for (int ps = 0; ps < rs.n; ++ps) {
-        if (ps == rs.n - 1) fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), sload, pix_dif);
-        else fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+        if (ps == rs.n - 1) fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, pix_dif);
+        else fft_pass_r<1, true>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
       }
     } else {
       for (int ps = 0; ps < rs.n - 1; ++ps)
-        fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+        fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
       const int R = rs.r(rs.n - 1);
       if (rs.n == 1) {
-        bluestein_mid(fx, R, F, +1, sload, pix_blue);
+        bluestein_mid(fx, R, F, +1, 0, sload, pix_blue);
       } else {
-        bluestein_mid(fx, R, F, +1, sload, sstore);
+        bluestein_mid(fx, R, F, +1, rs.wl(rs.n - 1), sload, sstore);
         for (int ps = rs.n - 2; ps >= 0; --ps) {
-          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, pix_blue);
-          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+          if (rs.wl(ps) == 0 && rs.wl(ps + 1) != 0) __syncthreads();
+          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), 0, sload, pix_blue);
+          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
         }
       }
     }
+    __syncthreads();  // the buffer is free for the other hemisphere
   }
 }
 
@@ -568,7 +612,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   phase_tables(plo, phi, p, c.ring);
   const int64_t half = p.nvecs, qstride = 2 * half;
   double *qbase = p.q_out + (int64_t)c.ring * (p.mmax + 1) * qstride + 2 * c.map0;
-  const Radices rs = radices(M);
+  const auto rs = radices<false>(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
   const double inv = c.pow2 ? 1.0 : 1.0 / (double)M;
@@ -601,22 +645,24 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
     };
     if (c.pow2) {
       for (int ps = rs.n - 1; ps >= 0; --ps) {
-        if (ps == rs.n - 1) fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), pix_dit, sstore);
-        else fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+        if (ps < rs.n - 1 && rs.wl(ps) == 0 && rs.wl(ps + 1) != 0) __syncthreads();
+        if (ps == rs.n - 1) fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), pix_dit, sstore);
+        else fft_pass_r<-1, false>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
       }
     } else {
       for (int ps = 0; ps < rs.n - 1; ++ps) {
-        if (ps == 0) fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), pix_blue, sstore);
-        else fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+        if (ps == 0) fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), 0, pix_blue, sstore);
+        else fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
       }
       const int R = rs.r(rs.n - 1);
       if (rs.n == 1) {
-        bluestein_mid(fx, R, F, -1, pix_blue, zstore);
+        bluestein_mid(fx, R, F, -1, 0, pix_blue, zstore);
       } else {
-        bluestein_mid(fx, R, F, -1, sload, sstore);
+        bluestein_mid(fx, R, F, -1, rs.wl(rs.n - 1), sload, sstore);
         for (int ps = rs.n - 2; ps >= 0; --ps) {
-          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, zstore);
-          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+          if (rs.wl(ps) == 0 && rs.wl(ps + 1) != 0) __syncthreads();
+          if (ps == 0) fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), 0, sload, zstore);
+          else fft_pass_r<1, false>(fx, rs.r(ps), rs.lgl(ps), rs.wl(ps), sload, sstore);
         }
       }
     }
@@ -713,10 +759,10 @@ __global__ void __launch_bounds__(kRingThreads) k_bluestein_filters(RingParams p
   __syncthreads();
   auto sload = [&](int i, int g) -> cplx { return buf[at(i, g, 0)]; };
   auto sstore = [&](int i, int g, cplx v) { buf[at(i, g, 0)] = v; };
-  const Radices rs = radices(M);
+  const auto rs = radices<true>(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, 0};
   for (int ps = 0; ps < rs.n; ++ps)
-    fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), sload, sstore);
+    fft_pass_r<-1, true>(fx, rs.r(ps), rs.lgl(ps), 0, sload, sstore);
   cplx *F = reinterpret_cast<cplx *>(p.filters_out) + R.filter;
   for (int k = threadIdx.x; k < M; k += blockDim.x) F[k] = buf[at(k, 0, 0)];
 }
