@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--eps", type=float, default=1e-10)
     ap.add_argument("--chunk", type=int, default=64)
     ap.add_argument("--memop", type=float, default=20.0)
+    ap.add_argument("--max-levels", type=int, default=1,
+                    help="cap on the interpolation levels of the plan files this script writes: 1 keeps "
+                         "every matrix on the tensor-core paths (trees of depth 0 and 1); -1: the "
+                         "writer's cost model over all levels")
     ap.add_argument("--plan-dir", default=os.environ.get("WAVEMOTH_PLAN_DIR",
                                                          os.path.join(ROOT, ".plan_cache")))
     ap.add_argument("--cpu-baseline-seconds", type=float, default=15.0)
@@ -85,9 +89,15 @@ def log(*args):
 
 # --------------------------------------------------------------------- plan
 
+def plan_levels(a):
+    lv = getattr(a, "max_levels", None)
+    return None if lv is None or lv < 0 else lv
+
+
 def plan_path(a):
-    return os.path.join(a.plan_dir, "rev1_nside%d_lmax%d_eps%g_chunk%d_memop%g.dat"
-                        % (a.nside, a.lmax, a.eps, a.chunk, a.memop))
+    lv = "" if plan_levels(a) is None else "_levels%d" % plan_levels(a)
+    return os.path.join(a.plan_dir, "rev1_nside%d_lmax%d_eps%g_chunk%d_memop%g%s.dat"
+                        % (a.nside, a.lmax, a.eps, a.chunk, a.memop, lv))
 
 
 def ensure_plan(a, rank):
@@ -100,7 +110,7 @@ def ensure_plan(a, rank):
         t = time.time()
         log("writing plan file %s ..." % path)
         resource.compute_resource_file(path, a.nside, a.lmax, chunk_size=a.chunk, eps=a.eps,
-                                       memop_cost=a.memop)
+                                       memop_cost=a.memop, max_levels=plan_levels(a))
         log("plan written in %.1f s" % (time.time() - t))
         return path
     deadline = time.time() + 1800
@@ -699,8 +709,8 @@ def run_b200(a):
                                  if a.precision == "split" else "plain FP64"),
                    "plain_fp64": plain,
                    "parity_vs_reference": parity,
-                   "plan": {"eps": a.eps, "chunk": a.chunk,
-                                                       "memop_cost": a.memop},
+                   "plan": {"eps": a.eps, "chunk": a.chunk, "memop_cost": a.memop,
+                            "max_levels": plan_levels(a)},
                    "parallelism": "replicas (maps sharded per GPU)" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (alm %.2f GB, maps %.2f GB per GPU)"
                          % (alm_h.nbytes / 1e9, T.npix * a.nmaps * 8 / 1e9)},
@@ -767,7 +777,7 @@ def run_uneven(a):
         n2048 += nside >= 2048
         nmaps = int(rng.integers(1, 9))
         pa = types.SimpleNamespace(nside=nside, lmax=2 * nside, eps=a.eps, chunk=a.chunk, memop=a.memop,
-                                   plan_dir=a.plan_dir)
+                                   plan_dir=a.plan_dir, max_levels=a.max_levels)
         # nside 2048 regenerates its residual P at every call: held sliced
         # (80 GB) it would leave no room for the other requests' images
         T = Transform(ensure_plan(pa, 0), nside, 2 * nside, nmaps,
@@ -818,6 +828,7 @@ def run_uneven(a):
                        "request_nsides": [T.nside for T in transforms],
                        "request_maps": [T.nmaps for T in transforms],
                        "request_precisions": [T.precision for T in transforms],
+                       "plan_max_levels": plan_levels(a),
                        "schedule": {"graph_branches": width, "sms_per_request": sms or "all",
                                     "search_seconds": tune_s},
                        "l2": "flushed between timed launches"},
@@ -840,7 +851,7 @@ def run_compare_dense(a):
     for nside in [int(x) for x in a.dense_nsides.split(",")]:
         lmax = 2 * nside
         pa = types.SimpleNamespace(nside=nside, lmax=lmax, eps=a.eps, chunk=a.chunk, memop=a.memop,
-                                   plan_dir=a.plan_dir)
+                                   plan_dir=a.plan_dir, max_levels=a.max_levels)
         path = ensure_plan(pa, 0)
         alm = torch.from_numpy(synthetic_alm(lmax, a.nmaps, 1000)).cuda()
         row = {"nside": nside, "lmax": lmax}

@@ -218,3 +218,24 @@ def test_config2_nside512_round_trip():
     p.close()
     assert np.abs(maps_s - maps).max() <= 1e-9 * np.abs(maps).max()
     assert np.abs(back_s - back).max() <= 1e-9 * np.abs(back).max()
+
+
+def test_depth_capped_plan_matches_reference_c():
+    """A plan file written with every matrix capped at one interpolation level
+    (the tensor-core paths' depth) against the reference C library on the
+    same file, and against the dense transform."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("reference C library not built")
+    nside, lmax, eps = 128, 256, 1e-10
+    path = plan_file(nside, lmax, 64, eps, 1e-10, workers=4, max_levels=1)
+    nmaps = 2
+    alm = osht.random_alm(lmax, nmaps, seed=11)
+    got, work = _alm2map_gpu(path, nside, lmax, alm)
+    rp = ref.RefPlan(nside, lmax, nmaps, path, nthreads=2)
+    rp.input[:] = alm
+    want = rp.execute().copy()
+    rp.close()
+    assert rel(got, want) < 1e-10
+    dense = osht.alm2map_dense(nside, alm, lmax)
+    assert rel(got, dense) < 10 * eps

@@ -576,12 +576,19 @@ class ResourceComputer:
     (lib.pyx:512-592)."""
 
     def __init__(self, nside, lmax, mmax, chunk_size=64, eps=1e-10, memop_cost=20.0,
-                 check_stability=True):
+                 check_stability=True, max_levels=None):
         if lmax != mmax:
             raise ValueError("only lmax == mmax is supported")
+        if max_levels is not None and max_levels < 0:
+            raise ValueError("max_levels must be None or >= 0")
         self.nside, self.lmax, self.mmax = nside, lmax, mmax
         self.chunk_size, self.eps, self.memop_cost = chunk_size, eps, memop_cost
         self.check_stability = check_stability
+        # None: every depth the tree has (the reference's choice); else the
+        # level choice stops at this many interpolation levels -- 1 keeps
+        # every matrix on this library's tensor-core paths, which run trees
+        # of depth 0 and 1 (deeper ones run on the generic FP64 kernels)
+        self.max_levels = max_levels
 
     def residual_cost(self, rows, cols):
         return rows * cols * (5.0 / 2.0 + 1) / self.memop_cost
@@ -591,6 +598,8 @@ class ResourceComputer:
         tree = butterfly_compress(provider, self.chunk_size,
                                   shape=(provider.nk, provider.ncols_full_matrix), eps=self.eps)
         depth = tree.get_max_depth()
+        if self.max_levels is not None:
+            depth = min(depth, self.max_levels)
         costs = np.zeros(depth + 1)
         for level in range(depth + 1):
             _, ip, res = tree.get_stats(level, self.residual_cost)
@@ -634,12 +643,14 @@ def _compute_one(rc, m, odd):
 
 
 def compute_resource_file(path, nside, lmax, mmax=None, chunk_size=64, eps=1e-10,
-                          memop_cost=20.0, max_workers=None):
-    """Write a rev1 plan file for (nside, lmax) to `path`; returns path."""
+                          memop_cost=20.0, max_workers=None, max_levels=None):
+    """Write a rev1 plan file for (nside, lmax) to `path`; returns path.
+    max_levels caps the interpolation levels of every matrix (None: the
+    cost model's choice over all of them)."""
     mmax = lmax if mmax is None else mmax
     if max_workers is None:
         max_workers = min(32, len(os.sched_getaffinity(0)))
-    rc = ResourceComputer(nside, lmax, mmax, chunk_size, eps, memop_cost)
+    rc = ResourceComputer(nside, lmax, mmax, chunk_size, eps, memop_cost, max_levels=max_levels)
     tmp = path + ".tmp%d" % os.getpid()
     with open(tmp, "wb") as f:
         rc.compute(f, max_workers=max_workers)
