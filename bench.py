@@ -830,7 +830,8 @@ def run_uneven(a):
                        "request_precisions": [T.precision for T in transforms],
                        "plan_max_levels": plan_levels(a),
                        "schedule": {"graph_branches": width, "sms_per_request": sms or "all",
-                                    "search_seconds": tune_s},
+                                    "search_seconds": tune_s,
+                                    "transforms_after_coalescing": B.transforms()},
                        "l2": "flushed between timed launches"},
             "clocks": clk,
             "sequential": {"value": total_maps / (seq_ms / 1e3), "unit": "maps/s", "ms_per_step": seq_ms}}

@@ -84,8 +84,13 @@ int wavemoth_execute_map2alm_device(wavemoth_plan plan, const double *map, doubl
    creation waits for `stream`, captures the requests, longest first, onto
    1, 2, 4 or 8 (at most max_width; <= 0 for 8) parallel graph branches,
    times each graph on a private stream (this runs every request a few
-   times) and keeps the fastest.  Creation must not run inside another
-   stream capture. */
+   times) and keeps the fastest.  Requests of one direction whose plans
+   share a device image (same plan file, lmax, precision and settings,
+   device pointers, no ring weights) run as one transform of their summed
+   map count, on a plan and interleaved buffers the batch allocates here and
+   frees with it; the graph gathers their inputs and scatters the results,
+   which equal those of the separate calls.  Creation must not run inside
+   another stream capture. */
 typedef struct _wavemoth_batch *wavemoth_batch;
 wavemoth_batch wavemoth_batch_create(int nreq, const wavemoth_plan *plans, const int *directions,
                                      const double *const *inputs, double *const *outputs,
@@ -105,6 +110,8 @@ wavemoth_batch wavemoth_batch_create_scheduled(int nreq, const wavemoth_plan *pl
 int wavemoth_batch_schedule(wavemoth_batch batch, int *width, int *sms, double *ms);
 /* The branch count the creation chose and its measured time per launch. */
 int wavemoth_batch_info(wavemoth_batch batch, int *width, double *ms);
+/* Transforms the batch's graph runs after coalescing (<= the requests). */
+int wavemoth_batch_transforms(wavemoth_batch batch);
 void wavemoth_batch_destroy(wavemoth_batch batch);
 
 /* The alm2map Legendre step of `plan` (q = A^T a for every (m, parity)),

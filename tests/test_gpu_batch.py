@@ -74,6 +74,47 @@ def test_uneven_batch_matches_single_calls():
         r[0].close()
 
 
+def test_same_shape_requests_coalesce():
+    """Requests of one direction on one plan file, lmax and precision run as
+    one transform of their summed maps (gathered and scattered inside the
+    graph); every request's output equals its single call bit for bit."""
+    from wavemoth_b200.batch import Batch
+    rng = np.random.default_rng(77)
+    specs = [(32, 1, "split", "alm2map"), (16, 2, "double", "map2alm"), (32, 3, "split", "alm2map"),
+             (32, 2, "double", "alm2map"), (16, 1, "double", "map2alm"), (32, 2, "split", "alm2map")]
+    reqs, singles = [], []
+    for i, (nside, nmaps, prec, direction) in enumerate(specs):
+        T = _transform(nside, nmaps, prec)
+        if direction == "alm2map":
+            inp = torch.from_numpy(osht.random_alm(T.lmax, nmaps, seed=700 + i)).cuda()
+            out = torch.full((T.npix, nmaps), float("nan"), dtype=torch.float64, device="cuda")
+            single = T.alm2map(inp).clone()
+        else:
+            inp = torch.from_numpy(rng.standard_normal((T.npix, nmaps))).cuda()
+            out = torch.full((T.nalm, nmaps), complex(float("nan"), float("nan")), dtype=torch.complex128,
+                             device="cuda")
+            single = T.map2alm(inp).clone()
+        reqs.append((T, direction, inp, out))
+        singles.append(single)
+    import tempfile
+    B = Batch(reqs, cache=tempfile.mktemp(prefix="wm_sched_", suffix=".json"))
+    # three transforms: split alm2map at nside 32 (6 maps), double map2alm at
+    # nside 16 (3 maps), double alm2map at nside 32
+    assert B.transforms() == 3
+    for _ in range(2):
+        for r in reqs:
+            r[3].fill_(float("nan"))
+        B.execute()
+        torch.cuda.synchronize()
+        for r, s in zip(reqs, singles):
+            assert torch.equal(r[3], s)
+    for r in reqs:
+        r[0].device_status()
+    B.close()
+    for r in reqs:
+        r[0].close()
+
+
 def test_batch_rejects_shared_transform():
     from wavemoth_b200.batch import Batch
     T = _transform(8, 1, "double")

@@ -29,6 +29,7 @@ SIGNATURES = {
     "wavemoth_batch_create": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "wavemoth_batch_execute": (ctypes.c_int, [_vp, _vp]),
     "wavemoth_batch_info": (ctypes.c_int, [_vp, _vp, _vp]),
+    "wavemoth_batch_transforms": (ctypes.c_int, [_vp]),
     "wavemoth_batch_destroy": (None, [_vp]),
     "wavemoth_batch_create_scheduled": (_vp, [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "wavemoth_batch_schedule": (ctypes.c_int, [_vp, _vp, _vp, _vp]),

@@ -8,6 +8,11 @@ and precision; no two may use the same Transform (its buffers would race).
 Creation captures the requests, longest first, onto parallel graph
 branches; `execute()` is then one graph launch on torch's current stream.
 
+Requests of one direction whose Transforms share a device image (same
+plan file, lmax and precision) run as one transform of their summed maps:
+the matrices are streamed once for all of them (`transforms()` counts what
+the graph runs; the results equal the separate calls').
+
 Schedule autotuning: a schedule is the number of branches and, with more
 than one, the SMs each request's persistent Legendre kernels may occupy
 (the CTAs walking its (m, parity) tile list).  Every candidate (branches 1,
@@ -123,6 +128,14 @@ class Batch:
         w, sms, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         _native.lib().wavemoth_batch_schedule(self._batch, ctypes.byref(w), ctypes.byref(sms), ctypes.byref(ms))
         return w.value, sms.value, ms.value
+
+    def transforms(self):
+        """Transforms the graph runs: requests of one direction on one device
+        image are coalesced into one transform of their summed map count."""
+        n = _native.lib().wavemoth_batch_transforms(self._batch)
+        if n < 0:
+            raise WavemothError("batch transforms: " + last_error())
+        return n
 
     def info(self):
         """(number of parallel graph branches chosen, measured ms per launch)."""

@@ -13,6 +13,15 @@
 // timed, and the fastest is kept (wavemoth_b200.batch caches the choice per
 // batch signature).  Every execute is then one cudaGraphLaunch.
 //
+// Requests of one direction whose plans share a device image (same plan
+// file, lmax, precision and settings) are coalesced into one transform of
+// their summed map count: the matrices are streamed once for all of them.
+// The batch owns that transform's plan (on the same image) and its
+// interleaved input and output buffers; inside the graph a copy kernel
+// gathers the requests' inputs before it and scatters the outputs after it.
+// Every map's arithmetic is independent of the other maps', so the results
+// are those of the separate calls.
+//
 // The plans' own buffers (q, X, operand slices) are shared by all calls on
 // one plan, so a batch must not hold two requests on the same plan.
 #include <cuda_runtime.h>
@@ -22,22 +31,37 @@
 #include <string>
 #include <vector>
 
+#include "kernels.h"
 #include "wavemoth.h"
 #include "wavemoth_b200.h"
 
 namespace wm {
 int set_last_error(int code, const std::string &msg);
+bool plans_coalescible(wavemoth_plan a, wavemoth_plan b);
+wavemoth_plan plan_with_maps(wavemoth_plan P, int nmaps);
+void plan_sizes(wavemoth_plan P, int64_t *nalm, int64_t *npix);
 }
 
 struct _wavemoth_batch {
+  // a request merged into a coalesced transform: its buffers and its maps'
+  // place among the transform's
+  struct Member {
+    const double *in;
+    double *out;
+    int nmaps, offset;
+  };
   struct Req {
     wavemoth_plan plan;
     int direction;
     const double *in;
     double *out;
     double cost;
+    std::vector<Member> members;  // empty: the caller's own request
+    double *own_in = nullptr;     // coalesced: the batch's interleaved input
   };
   std::vector<Req> reqs;
+  std::vector<wavemoth_plan> owned_plans;
+  std::vector<double *> owned_buffers;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int width = 0;
@@ -47,12 +71,15 @@ struct _wavemoth_batch {
   ~_wavemoth_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    for (auto p : owned_plans) wavemoth_destroy_plan(p);
+    for (auto b : owned_buffers) cudaFree(b);
   }
 };
 
 namespace {
 
 int capture_branches(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGraph_t *out);
+int run_request(const _wavemoth_batch::Req &r, cudaStream_t st);
 
 int cuda_err(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return 0;
@@ -66,6 +93,34 @@ int capture(_wavemoth_batch &B, int width, int sms, cudaStream_t origin, cudaGra
   for (const auto &r : B.reqs) wavemoth_plan_set_grid_cap(r.plan, width > 1 ? sms : 0);
   const int rc = capture_branches(B, width, origin, out);
   for (const auto &r : B.reqs) wavemoth_plan_set_grid_cap(r.plan, 0);
+  return rc;
+}
+
+// One request on `st`: a coalesced one gathers its members' inputs (alm
+// rows of 2 doubles per map, map rows of 1) into the interleaved buffer,
+// runs, and scatters the outputs back.
+int run_request(const _wavemoth_batch::Req &r, cudaStream_t st) {
+  const bool a2m = r.direction == 0;
+  if (r.members.empty())
+    return a2m ? wavemoth_execute_alm2map_device(r.plan, r.in, r.out, st)
+               : wavemoth_execute_map2alm_device(r.plan, r.in, r.out, st);
+  int64_t nalm = 0, npix = 0;
+  wm::plan_sizes(r.plan, &nalm, &npix);
+  const int64_t ntot = wavemoth_plan_nmaps(r.plan);
+  const int64_t in_rows = a2m ? nalm : npix, out_rows = a2m ? npix : nalm;
+  const int64_t in_w = a2m ? 2 : 1, out_w = a2m ? 1 : 2;
+  int rc = 0;
+  for (const auto &m : r.members)
+    if (!rc)
+      rc = cuda_err(wm::launch_strided_copy(r.own_in + m.offset * in_w, ntot * in_w, m.in, m.nmaps * in_w,
+                                            m.nmaps * in_w, in_rows, st), "batch gather");
+  if (!rc)
+    rc = a2m ? wavemoth_execute_alm2map_device(r.plan, r.in, r.out, st)
+             : wavemoth_execute_map2alm_device(r.plan, r.in, r.out, st);
+  for (const auto &m : r.members)
+    if (!rc)
+      rc = cuda_err(wm::launch_strided_copy(m.out, m.nmaps * out_w, r.out + m.offset * out_w, ntot * out_w,
+                                            m.nmaps * out_w, out_rows, st), "batch scatter");
   return rc;
 }
 
@@ -91,8 +146,7 @@ int capture_branches(_wavemoth_batch &B, int width, cudaStream_t origin, cudaGra
     if (rc) break;
     const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
     load[b] += r.cost;
-    rc = r.direction == 0 ? wavemoth_execute_alm2map_device(r.plan, r.in, r.out, br[b])
-                          : wavemoth_execute_map2alm_device(r.plan, r.in, r.out, br[b]);
+    rc = run_request(r, br[b]);
   }
   for (int i = 0; i < width && !rc; ++i) {
     rc = cuda_err(cudaEventRecord(done[i], br[i]), "join");
@@ -157,14 +211,59 @@ wavemoth_batch create_batch(int nreq, const wavemoth_plan *plans, const int *dir
         delete B;
         return nullptr;
       }
+  }
+  // requests of one direction on one image, in request order
+  std::vector<std::vector<int>> groups;
+  for (int i = 0; i < nreq; ++i) {
+    bool placed = false;
+    for (auto &g : groups)
+      if (directions[g[0]] == directions[i] && wm::plans_coalescible(plans[g[0]], plans[i])) {
+        g.push_back(i);
+        placed = true;
+        break;
+      }
+    if (!placed) groups.push_back({i});
+  }
+  for (const auto &g : groups) {
+    _wavemoth_batch::Req r{plans[g[0]], directions[g[0]], inputs[g[0]], outputs[g[0]], 0.0, {}, nullptr};
+    if (g.size() > 1) {
+      int ntot = 0;
+      for (int i : g) {
+        r.members.push_back({inputs[i], outputs[i], wavemoth_plan_nmaps(plans[i]), ntot});
+        ntot += wavemoth_plan_nmaps(plans[i]);
+      }
+      r.plan = wm::plan_with_maps(plans[g[0]], ntot);
+      if (!r.plan) {
+        delete B;
+        return nullptr;
+      }
+      B->owned_plans.push_back(r.plan);
+      int64_t nalm = 0, npix = 0;
+      wm::plan_sizes(r.plan, &nalm, &npix);
+      const int64_t alm_d = 2 * nalm * ntot, map_d = npix * ntot;
+      double *in = nullptr, *out = nullptr;
+      const bool a2m = r.direction == 0;
+      if (cuda_err(cudaMalloc(&in, sizeof(double) * (a2m ? alm_d : map_d)), "batch buffers")) {
+        delete B;
+        return nullptr;
+      }
+      B->owned_buffers.push_back(in);
+      if (cuda_err(cudaMalloc(&out, sizeof(double) * (a2m ? map_d : alm_d)), "batch buffers")) {
+        delete B;
+        return nullptr;
+      }
+      B->owned_buffers.push_back(out);
+      r.in = r.own_in = in;
+      r.out = out;
+    }
     double w[12] = {0};
-    if (wavemoth_plan_work(plans[i], wavemoth_plan_nmaps(plans[i]), w) != 0) {
+    if (wavemoth_plan_work(r.plan, wavemoth_plan_nmaps(r.plan), w) != 0) {
       delete B;
       return nullptr;
     }
     // seconds-scale estimate: FP64 flops at 30 TF/s plus ring bytes at 1 TB/s
-    const double cost = w[0] / 30e12 + w[3] / 1e12;
-    B->reqs.push_back({plans[i], directions[i], inputs[i], outputs[i], cost});
+    r.cost = w[0] / 30e12 + w[3] / 1e12;
+    B->reqs.push_back(r);
   }
   std::stable_sort(B->reqs.begin(), B->reqs.end(),
                    [](const _wavemoth_batch::Req &a, const _wavemoth_batch::Req &b) { return a.cost > b.cost; });
@@ -176,8 +275,9 @@ wavemoth_batch create_batch(int nreq, const wavemoth_plan *plans, const int *dir
     delete B;
     return nullptr;
   }
+  const int ntr = (int)B->reqs.size();
   for (const auto &sc : schedules) {
-    const int width = std::max(1, std::min(sc.first, nreq)), sms = std::max(0, sc.second);
+    const int width = std::max(1, std::min(sc.first, ntr)), sms = std::max(0, sc.second);
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ex = nullptr;
     int rc = capture(*B, width, sms, st, &g);
@@ -242,6 +342,11 @@ int wavemoth_batch_schedule(wavemoth_batch batch, int *width, int *sms, double *
   if (sms) *sms = batch->sms;
   if (ms) *ms = batch->ms;
   return 0;
+}
+
+int wavemoth_batch_transforms(wavemoth_batch batch) {
+  if (!batch) return wm::set_last_error(WAVEMOTH_ERR_ARG, "NULL batch");
+  return (int)batch->reqs.size();
 }
 
 int wavemoth_batch_execute(wavemoth_batch batch, void *stream) {

@@ -186,6 +186,11 @@ struct RingParams {
   double2 *phases_out;
 };
 
+// rows x width doubles from src (row pitch spitch) to dst (row pitch dpitch)
+// (batch_copy.cu).
+cudaError_t launch_strided_copy(double *dst, int64_t dpitch, const double *src, int64_t spitch, int64_t width,
+                                int64_t rows, cudaStream_t st);
+
 cudaError_t launch_ring_synthesis(const RingParams &prm, cudaStream_t st);
 // y = a - b (n doubles), and y += x (n doubles): the steps of the iterative
 // map2alm between the transforms
