@@ -285,6 +285,8 @@ int wavemoth_check_resourcefile(char *filename, int Nside, int lmax, int64_t *ou
 /* Host-side numerical tools of the plan-file writer (no GPU needed). */
 int wm_host_legendre(int m, const double *theta, int ntheta, int lmax, double eps, double *out);
 void wm_host_recurrence_coefficients(int64_t m, int64_t lmin, int64_t nk, double *aux);
+void wm_host_recurrence_last_row(const double *x2, const double *P0, const double *P1, const double *aux,
+                                 int64_t nx, int64_t nk, double *out);
 int wm_host_interp_decomp(double *A, int m, int n, double eps, int *krank, int *perm,
                           double *proj);
 

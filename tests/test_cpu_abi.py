@@ -143,9 +143,8 @@ def test_interp_decomp_contract():
 def test_every_declared_function_has_a_ctypes_signature():
     """Every C entry point of include/*.h is typed in wavemoth_b200._abi (or
     _native): an untyped ctypes call would pass 64-bit pointers as C ints."""
-    from wavemoth_b200 import _abi
-    typed = set(_abi.SIGNATURES) | {"wm_host_legendre", "wm_host_recurrence_coefficients",
-                                    "wm_host_interp_decomp", "wavemoth_create_healpix_grid_info",
-                                    "wavemoth_free_grid_info"}
+    from wavemoth_b200 import _abi, _native
+    typed = set(_abi.SIGNATURES) | set(_native.HOST_SIGNATURES) | {"wavemoth_create_healpix_grid_info",
+                                                                   "wavemoth_free_grid_info"}
     missing = [n for n in declared_functions() if n not in typed]
     assert not missing, missing

@@ -121,3 +121,22 @@ def test_ring_weights_integrate_zonal_harmonics():
             q = 4 * np.pi / (12 * nside * nside) * np.sum(c * n * w * ylm)
             assert abs(q - (np.sqrt(4 * np.pi) if l == 0 else 0.0)) < 1e-12
         assert 0.9 < w.min() and w.max() < 1.15
+
+
+def test_native_recurrence_last_row_matches_numpy_loop():
+    """The plan writer's stability check (wm_host_recurrence_last_row) runs the
+    residual recurrence of src/legendre_transform.c.in:680-716 per column."""
+    import numpy as np
+    from wavemoth_b200 import _native
+    rng = np.random.default_rng(3)
+    m, lmin, nk, nx = 7, 9, 40, 33
+    aux = _native.recurrence_coefficients(m, lmin, nk)
+    x2 = rng.uniform(0, 1, nx)
+    P0, P1 = rng.standard_normal(nx), rng.standard_normal(nx)
+    pp, p = P0.copy(), P1.copy()
+    for k in range(2, nk):
+        al, be, ga = aux[3 * (k - 2):3 * (k - 2) + 3]
+        pp, p = p, (x2 + al) * be * p + ga * pp
+    got = _native.recurrence_last_row(x2, P0, P1, aux, nk)
+    assert np.allclose(got, p, rtol=1e-12, atol=0)
+    assert np.array_equal(_native.recurrence_last_row(x2, P0, P1, aux[:0], 1), P0)

@@ -23,15 +23,21 @@ class NativeLibraryMissing(RuntimeError):
     pass
 
 
+# ctypes signatures of the host tools of the plan-file writer
+HOST_SIGNATURES = {
+    "wm_host_legendre": (ctypes.c_int, [ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, c_double_p]),
+    "wm_host_recurrence_coefficients": (None, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                               c_double_p]),
+    "wm_host_recurrence_last_row": (None, [c_double_p, c_double_p, c_double_p, c_double_p, ctypes.c_int64,
+                                            ctypes.c_int64, c_double_p]),
+    "wm_host_interp_decomp": (ctypes.c_int, [c_double_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, c_int_p, c_int_p, c_double_p]),
+}
+
+
 def _declare(lib):
-    sig = {
-        "wm_host_legendre": (ctypes.c_int, [ctypes.c_int, c_double_p, ctypes.c_int, ctypes.c_int,
-                                            ctypes.c_double, c_double_p]),
-        "wm_host_recurrence_coefficients": (None, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
-                                                   c_double_p]),
-        "wm_host_interp_decomp": (ctypes.c_int, [c_double_p, ctypes.c_int, ctypes.c_int,
-                                                 ctypes.c_double, c_int_p, c_int_p, c_double_p]),
-    }
+    sig = HOST_SIGNATURES
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res
@@ -80,6 +86,18 @@ def recurrence_coefficients(m, lmin, nk):
         return np.zeros(0)
     out = np.empty(3 * (nk - 2), np.float64)
     lib().wm_host_recurrence_coefficients(int(m), int(lmin), int(nk), dptr(out))
+    return out
+
+
+def recurrence_last_row(x2, P0, P1, aux, nk):
+    """Row nk-1 of the three-term recurrence started from (P0, P1), per column."""
+    x2, P0, P1 = (np.ascontiguousarray(v, dtype=np.float64) for v in (x2, P0, P1))
+    aux = np.ascontiguousarray(aux, dtype=np.float64)
+    if aux.size < 3 * max(0, nk - 2):
+        raise ValueError("recurrence coefficients too short")
+    out = np.empty(x2.shape[0], np.float64)
+    lib().wm_host_recurrence_last_row(dptr(x2), dptr(P0), dptr(P1), dptr(aux) if aux.size else None,
+                                      x2.shape[0], int(nk), dptr(out))
     return out
 
 

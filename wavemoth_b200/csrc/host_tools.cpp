@@ -124,4 +124,25 @@ int wm_host_interp_decomp(double *A, int m, int n, double eps, int *krank_out, i
   return 0;
 }
 
+// Row nk - 1 of the three-term recurrence P_k = (x2 + alpha_k) beta_k P_{k-1}
+// + gamma_k P_{k-2} started from P0, P1 (aux: (alpha, beta, gamma) for k =
+// 2 .. nk - 1), for nx columns; the plan writer's stability check.
+void wm_host_recurrence_last_row(const double *x2, const double *P0, const double *P1, const double *aux,
+                                 int64_t nx, int64_t nk, double *out) {
+  for (int64_t j = 0; j < nx; ++j) {
+    double pp = P0[j], p = P1[j];
+    if (nk <= 1) {
+      out[j] = pp;
+      continue;
+    }
+    for (int64_t k = 2; k < nk; ++k) {
+      const double *a = aux + 3 * (k - 2);
+      const double nv = (x2[j] + a[0]) * a[1] * p + a[2] * pp;
+      pp = p;
+      p = nv;
+    }
+    out[j] = p;
+  }
+}
+
 }  // extern "C"

@@ -477,15 +477,6 @@ def stripify(A, include_above=1e-30, exclude_below=1e-80, jump_treshold=10, col_
     return strips
 
 
-def _recurrence_last_row(x2, P0, P1, aux, nk):
-    """Row nk-1 of the three-term recurrence started from (P0, P1)."""
-    pp, p = P0.copy(), P1.copy()
-    for k in range(2, nk):
-        al, be, ga = aux[3 * (k - 2):3 * (k - 2) + 3]
-        pp, p = p, (x2 + al) * be * p + ga * pp
-    return p if nk > 1 else pp
-
-
 class LegendreMatrixProvider:
     """Even (odd=0) or odd (odd=1) rows l = m + 2k + odd of Lambda_m, columns
     = the 2*nside northern rings from the equator (lib.pyx:376-395)."""
@@ -559,7 +550,7 @@ class LegendreMatrixProvider:
                 _aligned(stream, P0)
                 _aligned(stream, P1)
                 if self.check_stability:
-                    y = _recurrence_last_row(xs, P0, P1, aux[3 * rstart:], rstop - rstart)
+                    y = _native.recurrence_last_row(xs, P0, P1, aux[3 * rstart:], rstop - rstart)
                     ny = np.linalg.norm(y)
                     if ny > 0 and np.linalg.norm(y - Lam[-1, cstart:cstop]) / ny > 1e-9:
                         raise ArithmeticError("numerically unstable recurrence start "
