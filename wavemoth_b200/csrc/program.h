@@ -53,6 +53,11 @@ struct HostProgram {
   // (kStream* order); encoded kZeroBufShift-bit buffer (0 q, 1 X, 2 alm)
   // above the row index
   std::vector<int64_t> split_zero[4];
+  // per ring pair: 1 + the largest m for which the ring's Legendre column
+  // (either parity) has a value above the plan writer's inclusion threshold
+  // 1e-30; the q rows of larger m hold at most 1e-30 |a|, and the synthesis
+  // gather of an alm2map stops there (empty: no limit)
+  std::vector<int32_t> ring_mend;
   // algorithmic work of one transform direction
   int64_t interp_elems = 0;      // sum of k (n - k) over interpolation blocks
   int64_t rec_elems = 0;         // recurrence-strip elements (rows x columns)

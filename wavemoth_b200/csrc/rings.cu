@@ -494,6 +494,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
   // q rows are ring-major: (m, parity) of ring r at row (r (mmax + 1) + m) 2 + parity
   const int64_t half = p.nvecs, qstride = 2 * half;
   const double *qbase = p.q + (int64_t)c.ring * (p.mmax + 1) * qstride + 2 * c.map0;
+  // the aliasing sums stop at the ring's m limit (null: every m)
+  const int mlim = p.ring_mend ? p.ring_mend[c.ring] - 1 : p.mmax;
   const auto rs = radices<false>(M);
   const FftCtx fx{p.twiddles, ilog2(p.twlen), M, lg};
   const cplx *F = reinterpret_cast<const cplx *>(p.filters) + c.R.filter;
@@ -510,8 +512,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
       const int mi = t & gmm, kk = t >> c.lgm;
       const bool live = t < nitems && mi < c.nm;
       const double *qg = qbase + 2 * mi;
-      first_term(qg, kk, p.mmax, qstride, half, live, qa[0], qb[0]);
-      first_term(qg, N - kk, p.mmax, qstride, half, live && N - kk != kk, qa[1], qb[1]);
+      first_term(qg, kk, mlim, qstride, half, live, qa[0], qb[0]);
+      first_term(qg, N - kk, mlim, qstride, half, live && N - kk != kk, qa[1], qb[1]);
     };
     cplx qa[2], qb[2];
     fetch(threadIdx.x, qa, qb);
@@ -523,8 +525,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_synthesis(RingParams p
         cplx Aa = {0.0, 0.0}, Ba = {0.0, 0.0}, Ab = {0.0, 0.0}, Bb = {0.0, 0.0};  // at kk and N - kk
         if (mi < c.nm) {
           const double *qg = qbase + 2 * mi;
-          alias_sums(qg, kk, n, p.mmax, qstride, half, plo, phi, qa[0], qb[0], Aa, Ba);
-          if (kr != kk) alias_sums(qg, kr, n, p.mmax, qstride, half, plo, phi, qa[1], qb[1], Ab, Bb);
+          alias_sums(qg, kk, n, mlim, qstride, half, plo, phi, qa[0], qb[0], Aa, Ba);
+          if (kr != kk) alias_sums(qg, kr, n, mlim, qstride, half, plo, phi, qa[1], qb[1], Ab, Bb);
           else { Ab = Aa; Bb = Ba; }
         }
 #pragma unroll
