@@ -160,7 +160,8 @@ struct RingParams {
   int32_t nmaps;
   int32_t nvecs;
   const double *q;        // synthesis input: rows of nvecs doubles, (m, parity) of ring r at (r (mmax + 1) + m) 2 + parity
-  const int32_t *ring_mend;  // synthesis: per ring pair, the aliasing sums stop below m = ring_mend[r] (null: mmax + 1)
+  const int32_t *ring_mend;  // per ring pair m limit (null: mmax + 1): synthesis sums m < ring_mend[r],
+                             // analysis writes zero q~ rows from there on
   double *map;            // synthesis output (npix, nmaps)
   const double *map_in;   // analysis input (npix, nmaps)
   double *q_out;          // analysis output

@@ -622,6 +622,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
   const bool npow2 = (n & (n - 1)) == 0;  // every belt ring when nside is a power of two
   // 4 pi / npix, times the ring's quadrature weight when weights are set
   const double wscale = p.ring_weights ? p.scale * p.ring_weights[c.ring] : p.scale;
+  // rows above the ring's m limit are written as zeros (null: every m folded)
+  const int mlim = p.ring_mend ? p.ring_mend[c.ring] - 1 : p.mmax;
   for (int side = 0; side < (c.two ? 1 : 2); ++side) {
     if (side == 1 && c.ring == 0) break;
     auto in_row = [&](int g, int64_t pix) -> const double * {
@@ -689,6 +691,14 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_ring_analysis(RingParams p)
       if (mi >= c.nm) continue;
       double *qe = qbase + m * qstride + 2 * mi;
       double *qo = qe + half;
+      if (m > mlim) {
+        // the Legendre step weighs these q~ rows by values below 1e-30
+        if (c.two || side == 0) {
+          st2(qe, 0.0, 0.0);
+          st2(qo, 0.0, 0.0);
+        }
+        continue;
+      }
       if (c.two) {
         // both hemispheres: q~_even = g_N + g_S, q~_odd = g_N - g_S (g_S = 0 at the equator)
         const cplx gN = fold(m, mi), gS = fold(m, (1 << c.lgm) | mi);
